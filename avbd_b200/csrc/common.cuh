@@ -1,0 +1,260 @@
+// Shared device definitions for the B200 Solver6DOF substep.
+//
+// Data model (see DESIGN.md for the full table):
+//  * bodies are SoA float4 arrays (x.xyz + mass, q, v, w, ...);
+//  * constraints are stored as *contact groups*: a normal row plus its two
+//    friction rows (floor corner or box-box contact), a 1-row frictionless
+//    contact, or the three axis rows of a pin.  A group's rows share bodies
+//    and anchors, so the primal reads the geometry once for up to three rows.
+//    The reference's row numbering (c_* arrays, solver_6dof.py:1067-1129) is
+//    kept through g_row0, so row-indexed API results are unchanged.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/avbd6.h"
+
+namespace avbd {
+
+// Group kinds.  The row types they carry are those of solver_6dof.py:31-34.
+enum : int { KIND_FLOOR = 0, KIND_PIN = 1, KIND_BOX = 2 };
+// g_meta bit layout.
+//   bits 0-1 kind, bit 2: three rows (else one), bit 3: hard (stiffness=inf),
+//   bits 4-5 contact ordinal within the pair manifold (box groups).
+__host__ __device__ inline int meta_kind(int m) { return m & 3; }
+__host__ __device__ inline int meta_nrows(int m) { return (m & 4) ? 3 : 1; }
+__host__ __device__ inline bool meta_hard(int m) { return (m & 8) != 0; }
+__host__ __device__ inline int meta_cidx(int m) { return (m >> 4) & 3; }
+__host__ __device__ inline int make_meta(int kind, int three, int hard, int cidx) {
+  return kind | (three ? 4 : 0) | (hard ? 8 : 0) | (cidx << 4);
+}
+// g_flags bit layout: bits 0-2 row active, bit 3 normal row was_static,
+// bits 4/5 the friction rows' own was_static (carried to the cache).
+enum : int { FL_ACT0 = 1, FL_ACT1 = 2, FL_ACT2 = 4, FL_WAS = 8, FL_WAST = 16, FL_WASB = 32 };
+
+// Penalty constants: kernels_6dof.py:50-52.
+#define PEN_MIN 1.0e6f
+#define PEN_MIN_T 1.0f
+#define PEN_MAX 1.0e9f
+#define MAX_COLORS 32
+#define JP_ROUNDS 24
+#define COLL_MARGIN 0.005f
+
+// Error bits of the device status word.
+enum : int {
+  ERR_BARRIER_TIMEOUT = 1,
+  ERR_HASH_FULL = 2,
+  ERR_PAIR_OVERFLOW = 4,
+  ERR_ROW_OVERFLOW = 8,
+  ERR_NONFINITE = 16,
+  ERR_NBR_OVERFLOW = 32,
+  ERR_BVH = 64,
+};
+
+// Counters written on the device, read by the host once per frame.
+struct DevCounters {
+  int n_pairs_found;     // canonical (i<j) broadphase pairs found this substep
+  int n_nbr_found;       // directed neighbour entries found (2 * pairs)
+  int n_pairs;           // pairs kept (<= pair_cap)
+  int n_dyn_groups;      // dynamic contact groups kept
+  int n_dyn_rows;        // dynamic rows kept
+  int n_dyn_rows_req;    // dynamic rows requested (may exceed capacity)
+  int n_contacts_req;    // contacts found by the manifold
+  int n_colors;          // active colors
+  int recolored;         // 1 if the last substep recolored
+  int conflicts;         // same-color edges seen by the recolor gate
+  int uncolored;         // scratch for the coloring convergence test
+  int color_dirty;       // host request: force a recolor on the next substep
+  int err;               // error bits (ERR_*)
+  int err_where;         // barrier index of a timeout
+  unsigned epoch;        // contact-cache epoch (substeps since the last clear)
+  int n_cache_hits;      // warm-start cache hits in the last emission
+  int n_new_contacts;    // cache misses in the last emission
+  int max_dg;            // longest per-body dynamic incidence list
+  unsigned viol_bits[64];  // per-iteration max violation (float bits, >= 0)
+  int n_viol;
+  int pad[15];
+  // grid barrier state (kept on its own 128-byte lines)
+  unsigned bar_count;
+  unsigned pad2[31];
+  unsigned bar_gen;
+  unsigned pad3[31];
+};
+
+// Scalars read by the kernels from device memory, so a captured graph sees
+// parameter changes without being re-captured.
+struct DevParams {
+  float dt;  // substep dt
+  int iterations;
+  float gx, gy, gz;
+  float alpha, beta, gamma;
+  int post_stab;
+  float max_lin, max_ang;  // +inf when the cap is off
+  float fsm;
+  int color_mode;  // 0 jacobi, 1 jones-plassmann
+  int recolor_every;
+  float self_friction;
+  int group_size;
+  int record_violation;
+  int debug_skip_arrive;
+  int mlp_on;
+  unsigned long long barrier_timeout_ns;
+  int pad[8];
+};
+
+// Every device pointer and size one substep needs.  Passed by value.
+struct Dev {
+  const DevParams* prm;
+  // sizes
+  int nb, n_sg, n_static_rows, g_cap, row_cap, pair_cap, nbr_cap, hash_cap;
+  int n_sg_rows_unused;
+  // bodies
+  float4 *x, *q, *v, *w, *pv, *pw, *x0, *q0, *xin, *qin, *iw0, *iw1, *iloc, *he;
+  float* prio;
+  int *color, *color2, *color_starts, *color_bodies;
+  int *sg_start;
+  int *dg_start, *dg_cnt, *dg_idx;
+  // groups
+  int2* g_body;
+  int *g_meta, *g_row0, *g_flags;
+  float4 *g_offa, *g_offb, *g_n, *g_mat, *g_lam, *g_pen, *g_ac0;
+  // broad phase
+  float4 *aabb_lo, *aabb_hi;
+  unsigned *morton, *morton2;
+  int *order, *order2;
+  float4 *node_lo, *node_hi;
+  int *node_left, *node_right, *node_parent, *node_flag;
+  float* bounds;  // 6 floats (lo xyz, hi xyz) as ordered ints
+  int *nbr_cnt, *nbr_start, *nbr_idx, *nbr_pair;
+  int *up_cnt, *pair_start;
+  int2* pair_ab;
+  int* pair_info;     // overlap | sat_idx<<1 | count<<6 | ref_is_a<<9
+  float4* pair_nrm;   // manifold normal (inc -> ref), w = SAT depth
+  float4* pair_off;   // 8 per pair: off_ref[4], off_inc[4]
+  int *pair_gcnt, *pair_gstart, *pair_rstart, *pair_kept;
+  // contact cache
+  unsigned long long* h_key;
+  float4 *h_s0, *h_s1;
+  // scan scratch
+  int* scan_part;
+  int scan_part_cap;
+  // radix sort scratch
+  int* sort_hist;
+  // coloring scratch
+  int *c_used, *c_lost, *c_hist;
+  // learned warm start (optional): packed weights, null when disabled
+  const float* mlp_w;
+  // counters
+  DevCounters* ctr;
+};
+
+// ---------------------------------------------------------------------------
+// Small vector / quaternion math (float).  Quaternions are XYZW.
+// ---------------------------------------------------------------------------
+struct V3 {
+  float x, y, z;
+};
+__host__ __device__ __forceinline__ V3 mk(float a, float b, float c) { return V3{a, b, c}; }
+__host__ __device__ __forceinline__ V3 xyz(float4 a) { return V3{a.x, a.y, a.z}; }
+__host__ __device__ __forceinline__ V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__host__ __device__ __forceinline__ V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__host__ __device__ __forceinline__ V3 operator-(V3 a) { return V3{-a.x, -a.y, -a.z}; }
+__host__ __device__ __forceinline__ V3 operator*(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+__host__ __device__ __forceinline__ V3 operator/(V3 a, float s) { return V3{a.x / s, a.y / s, a.z / s}; }
+__host__ __device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ __forceinline__ V3 cross(V3 a, V3 b) {
+  return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__host__ __device__ __forceinline__ float comp(V3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+
+// Hamilton product.
+__device__ __forceinline__ float4 qmul(float4 a, float4 b) {
+  return make_float4(a.w * b.x + b.w * a.x + (a.y * b.z - a.z * b.y), a.w * b.y + b.w * a.y + (a.z * b.x - a.x * b.z),
+                     a.w * b.z + b.w * a.z + (a.x * b.y - a.y * b.x), a.w * b.w - (a.x * b.x + a.y * b.y + a.z * b.z));
+}
+__device__ __forceinline__ float4 qconj(float4 q) { return make_float4(-q.x, -q.y, -q.z, q.w); }
+// v' = (2w^2-1) v + 2 (q.v) q + 2 w (q x v)
+__device__ __forceinline__ V3 qrot(float4 q, V3 v) {
+  float c = 2.0f * q.w * q.w - 1.0f;
+  float d = 2.0f * (q.x * v.x + q.y * v.y + q.z * v.z);
+  float w2 = q.w * 2.0f;
+  return V3{v.x * c + q.x * d + (q.y * v.z - q.z * v.y) * w2, v.y * c + q.y * d + (q.z * v.x - q.x * v.z) * w2,
+            v.z * c + q.z * d + (q.x * v.y - q.y * v.x) * w2};
+}
+struct M3 {
+  float m[3][3];
+};
+__host__ __device__ __forceinline__ M3 qmat(float4 q) {
+  float x = q.x, y = q.y, z = q.z, w = q.w;
+  M3 R;
+  R.m[0][0] = 1.0f - 2.0f * (y * y + z * z);
+  R.m[0][1] = 2.0f * (x * y - z * w);
+  R.m[0][2] = 2.0f * (x * z + y * w);
+  R.m[1][0] = 2.0f * (x * y + z * w);
+  R.m[1][1] = 1.0f - 2.0f * (x * x + z * z);
+  R.m[1][2] = 2.0f * (y * z - x * w);
+  R.m[2][0] = 2.0f * (x * z - y * w);
+  R.m[2][1] = 2.0f * (y * z + x * w);
+  R.m[2][2] = 1.0f - 2.0f * (x * x + y * y);
+  return R;
+}
+__host__ __device__ __forceinline__ V3 mcol(const M3& R, int k) { return V3{R.m[0][k], R.m[1][k], R.m[2][k]}; }
+__host__ __device__ __forceinline__ V3 mtv(const M3& R, V3 v) {
+  return V3{R.m[0][0] * v.x + R.m[1][0] * v.y + R.m[2][0] * v.z, R.m[0][1] * v.x + R.m[1][1] * v.y + R.m[2][1] * v.z,
+            R.m[0][2] * v.x + R.m[1][2] * v.y + R.m[2][2] * v.z};
+}
+
+// Rotation vector -> unit quaternion: kernels_6dof.py:63-73.
+__device__ __forceinline__ float4 quat_from_rotvec(V3 rv) {
+  float th = sqrtf(dot(rv, rv));
+  if (th < 1.0e-9f) return make_float4(0.5f * rv.x, 0.5f * rv.y, 0.5f * rv.z, 1.0f);
+  float s, c;
+  sincosf(0.5f * th, &s, &c);
+  s = s / th;
+  return make_float4(s * rv.x, s * rv.y, s * rv.z, c);
+}
+// Unit quaternion -> rotation vector in [-pi, pi]: kernels_6dof.py:76-97.
+__device__ __forceinline__ V3 quat_to_rotvec(float4 q) {
+  if (q.w < 0.0f) q = make_float4(-q.x, -q.y, -q.z, -q.w);
+  V3 qv{q.x, q.y, q.z};
+  float l = sqrtf(dot(qv, qv));
+  if (l < 1.0e-9f) return V3{0.0f, 0.0f, 0.0f};
+  float ang = 2.0f * atan2f(l, q.w);
+  return qv * (ang / l);
+}
+__device__ __forceinline__ float4 qnormalize(float4 q) {
+  float l = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+  if (l > 0.0f) {
+    float s = 1.0f / l;
+    return make_float4(q.x * s, q.y * s, q.z * s, q.w * s);
+  }
+  return q;
+}
+
+// Duff et al. 2017 tangent of n: kernels_6dof.py:2208-2218.
+__host__ __device__ __forceinline__ V3 orthonormal_basis(V3 n) {
+  float sign = n.z >= 0.0f ? 1.0f : -1.0f;
+  float a = -1.0f / (sign + n.z);
+  float b = n.x * n.y * a;
+  return V3{1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x};
+}
+
+// 64-bit contact-cache key (a < b, ordinal c).  The epoch tag lives in bits
+// 50-63 of the stored slot.
+__host__ __device__ __forceinline__ unsigned long long cache_key(int a, int b, int c) {
+  return ((unsigned long long)(unsigned)a << 26) | ((unsigned long long)(unsigned)b << 2) | (unsigned long long)c;
+}
+#define KEY_MASK ((1ull << 50) - 1ull)
+__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z ^= z >> 31;
+  z *= 0x7fb5d329728ea185ull;
+  z ^= z >> 27;
+  z *= 0x81dadef4bc2dd44dull;
+  z ^= z >> 33;
+  return z;
+}
+__host__ __device__ __forceinline__ unsigned epoch_tag(unsigned epoch) { return 1u + (epoch % 16000u); }
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+}  // namespace avbd

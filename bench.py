@@ -1,0 +1,325 @@
+"""Benchmark: body-substeps/s of the Solver6DOF substep on the 100k-box pile.
+
+Workload (the metric's configuration): 100,000 OBBs, half extents uniform in
+[0.2, 0.4] m, random orientations, density 1000, on a 100x100x10 jittered
+grid (1.4 m spacing) over a floor, one box in 500 corner-pinned with a
+breakable pin (5e4 N); dt 1/60, 4 substeps, 10 iterations + post-stabilization,
+Jones-Plassmann coloring.  The pile is settled (untimed) before the warm-up so
+the timed frames run on a resting pile (~1M dynamic contact rows).
+
+A "step" is one frame (4 substeps).  value = bodies x substeps x steps / device
+time of the timed steps (CUDA events on the solver's stream, L2 flushed between
+steps outside the events); with torchrun, N independent replicas (one pile per
+GPU, no collective in the loop) and the max time over ranks.
+
+`--impl reference` times the CPU restatement of the reference algorithm (the
+reference's own Warp CPU path cannot be installed here) on all host cores, on a
+bounded sample of the workload (a 20x20x10 tile of the same pile distribution).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "body-substeps/s @100k boxes; iters to 1e-4 m violation, learned vs plain λ0"
+UNIT = "body-substeps/s"
+PARAMS = dict(dt=1.0 / 60.0, iterations=10, substeps=4, friction_static_mult=1.25, coloring_mode="jones_plassmann")
+FULL = dict(nx=100, nz=100, ny=10)
+SAMPLE = dict(nx=20, nz=20, ny=10)
+
+
+def dyn_bodies(s) -> int:
+    return int(sum(1 for m in s._mass if m > 0.0))
+
+
+# ---------------------------------------------------------------------------
+# Per-launch algorithmic bytes (the per-unit figures of the survey's
+# measurement section; units from the live counters of the same run).
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(n_bodies: int, r1: int, r2: int, n_pairs: int, pairs_with_contacts: int, contacts: int,
+                      iterations: int) -> dict:
+    T = iterations + 1
+    solve = (n_bodies * 184 + (r1 + r2) * (124 + 24) + T * (n_bodies * 112 + r1 * 44 + 2 * r2 * 84)
+             + (T - 1) * (r1 * 100 + r2 * 128) + n_bodies * 104 + contacts * 64)
+    collide = n_bodies * 64 + n_pairs * 108 + pairs_with_contacts * 140 + contacts * (3 * 72 + 40)
+    return {"solve": solve, "collide": collide, "substep": solve + collide}
+
+
+# ---------------------------------------------------------------------------
+# nvidia-smi clock sampler (runs during the timed region).
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (C++ restatement, OpenMP) on a tile of the pile.
+# ---------------------------------------------------------------------------
+def cpu_rate(steps: int, warmup: int, threads: int, settle: int = 120) -> dict:
+    from avbd_b200 import scenes
+    from oracle.oracle import OracleSolver6DOF
+    s = OracleSolver6DOF(precision="float32", threads=threads, **PARAMS)
+    scenes.pile(s, **SAMPLE)
+    for _ in range(settle + warmup):
+        s.step()
+    nb = dyn_bodies(s)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step()
+    dt = time.perf_counter() - t0
+    c = s.counts()
+    return {"value": nb * PARAMS["substeps"] * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"{SAMPLE['nx']}x{SAMPLE['nz']}x{SAMPLE['ny']} tile of the pile ({nb} boxes, "
+                       f"{c['n_rows'] - c['n_static']} dynamic rows), settled {settle} frames, "
+                       f"{steps} timed frames; FP32 C++ restatement of the reference substep"),
+            "seconds": dt}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    r = cpu_rate(args.steps, args.warmup, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / max(1, args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "pile (OBB pile, 4 substeps x (10+1) iterations, JP coloring): bounded tile sample",
+                       "sample": r["sample"]},
+            "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm.
+# ---------------------------------------------------------------------------
+def run_gpu(args) -> None:
+    import torch
+    import torch.distributed as dist
+    from avbd_b200 import Solver6DOF, scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    size = dict(FULL) if not args.small else dict(nx=40, nz=40, ny=10)
+    s = Solver6DOF(device=str(dev), **PARAMS)
+    if args.group_size:
+        s.primal_group_size = args.group_size
+    if args.blocks_per_sm:
+        s.blocks_per_sm = args.blocks_per_sm
+    scenes.pile(s, **size)
+    nb = dyn_bodies(s)
+    for _ in range(args.settle):
+        s._enqueue_step()
+    s._after_frame()
+    for _ in range(args.warmup):
+        s.step()
+    st0 = s.stats()
+    stream = s._cuda_stream
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    if args.profile:
+        torch.cuda.profiler.start()
+    k0 = s.stats()["kernels_launched"]
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[k][0].record(stream)
+        s._enqueue_step()
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+        s._after_frame()
+    barrier()
+    if args.profile:
+        torch.cuda.profiler.stop()
+    kernels = s.stats()["kernels_launched"] - k0
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    st = s.stats()
+    coll_ms, solve_ms = s.broadphase_ms, s.solve_ms
+
+    # end to end through the public API: pinned host state in, step, poses out
+    n = len(s._x)
+    pin_in = [torch.empty((n, 4), dtype=torch.float32).pin_memory() for _ in range(4)]
+    pin_out = [torch.empty((n, 4), dtype=torch.float32).pin_memory() for _ in range(2)]
+    with torch.cuda.stream(stream):
+        for h, t in zip(pin_in, (s.x4, s.q, s.v4, s.w4)):
+            h.copy_(t[:n], non_blocking=True)
+    stream.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.upload_body_state(*pin_in)
+        s.step()
+        s.download_poses(*pin_out)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    h2d = sum(int(t.numel() * 4) for t in pin_in)
+    d2h = sum(int(t.numel() * 4) for t in pin_out)
+
+    def red_max(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms = red_max(ms)
+    e2e_s = red_max(e2e_s)
+    units = nb * PARAMS["substeps"] * args.steps * world
+    value = units / (ms / 1e3)
+    e2e_value = units / e2e_s
+    r1 = len(s._rows)
+    r2 = int(st["n_dyn_rows"])
+    pairs_c = int(st["n_dyn_groups"] > 0)  # refined below from the pair list
+    p = s.pairs()
+    pairs_with = int(np.sum(p["count"] > 0))
+    ab = algorithmic_bytes(n, r1, r2, int(st["n_pairs"]), pairs_with, int(st["n_dyn_groups"]), PARAMS["iterations"])
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = ab["solve"] / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "solve_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("bytes_per_launch_scaled")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": (f"pile {size['nx']}x{size['nz']}x{size['ny']} ({nb} OBBs, he U[0.2,0.4], "
+                                f"{sum(1 for r in s._rows if r.type == 2) // 3} corner pins fracture 5e4), dt 1/60, "
+                                "4 substeps, 10 iterations + post-stab, JP coloring; settled "
+                                f"{args.settle} frames before warm-up"),
+                   "global_batch": nb * world, "seq_len": None, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MiB write) between timed steps, outside the events",
+                   "live": {"dyn_rows": r2, "static_rows": r1, "pairs": int(st["n_pairs"]),
+                            "contacts": int(st["n_dyn_groups"]), "colors": int(st["n_colors"])}},
+        "roofline": {"bound": "hbm", "kernel": "k_solve_persistent", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": ab["solve"], "launch_ms": solve_ms,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(kernels),
+        "clocks": clk,
+        "phase_ms_per_substep": {"collide": coll_ms, "solve": solve_ms},
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cb = cpu_rate(steps=3, warmup=1, threads=threads, settle=60)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--settle", type=int, default=240)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="40x40x10 pile (profiling captures)")
+    ap.add_argument("--profile", action="store_true", help="cudaProfilerStart/Stop around the timed steps")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--group-size", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+/*
+ * avbd6.h -- C ABI of libavbd6.so, the B200 (sm_100a) implementation of the
+ * Solver6DOF substep of nanli9/AVBD (package avbd3d).
+ *
+ * The reference drives its substep from Python through Warp launches
+ * (src/avbd3d/solver_6dof.py:1178-1464, kernels in src/avbd3d/kernels_6dof.py).
+ * This library replaces that whole launch sequence.  Conventions:
+ *
+ *  - Memory: the caller owns every device buffer.  The library describes one
+ *    device arena (avbd_layout: byte offset of each array); the caller
+ *    allocates it (PyTorch in the shipped host code), fills the scene arrays
+ *    and passes the base pointer to avbd_create.  The library allocates only
+ *    its context and CUDA graph objects.  An arena must not be freed or moved
+ *    while a context uses it.
+ *  - Errors: every call returns 0 or a negative AVBD_E_* code; the device
+ *    status bits (AVBD_ERR_*) are reported through avbd_read_stats.
+ *  - Streams: `stream` is a cudaStream_t passed as void*; calls enqueue work
+ *    asynchronously except avbd_read_stats (synchronises the stream).
+ *  - Threads: one context per host thread at a time.
+ */
+#ifndef AVBD6_H
+#define AVBD6_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AVBD_OK 0
+#define AVBD_E_INVALID -1    /* bad argument or size */
+#define AVBD_E_CUDA -2       /* a CUDA call failed */
+#define AVBD_E_TIMEOUT -3    /* a bounded device wait ran out */
+#define AVBD_E_OVERFLOW -4   /* a pool overflowed (contacts dropped) */
+
+/* Device status bits (AvbdStats.err). */
+#define AVBD_ERR_BARRIER_TIMEOUT 1
+#define AVBD_ERR_HASH_FULL 2
+#define AVBD_ERR_PAIR_OVERFLOW 4
+#define AVBD_ERR_ROW_OVERFLOW 8
+#define AVBD_ERR_NONFINITE 16
+#define AVBD_ERR_NBR_OVERFLOW 32
+#define AVBD_ERR_BVH 64
+
+/* Sizes that fix the arena layout.  Mirrors the capacities the reference
+ * sizes in Solver6DOF._flush (solver_6dof.py:937-943, 1150-1163). */
+typedef struct AvbdDims {
+  int n_bodies;
+  int n_static_groups; /* floor corners, pins: fixed at scene build */
+  int n_static_rows;   /* rows of those groups (reference row numbering) */
+  int pair_cap;        /* broadphase pairs i<j (reference _bp_max_pairs) */
+  int dyn_row_cap;     /* dynamic contact rows (reference n_dyn_capacity) */
+  int dyn_group_cap;   /* dynamic contact groups (<= dyn_row_cap) */
+  int hash_cap;        /* contact-cache slots, power of two */
+  int mlp_floats;      /* learned warm-start weights (0 = none) */
+} AvbdDims;
+
+/* Scalars of Solver6DOF.__init__ (solver_6dof.py:180-201). */
+typedef struct AvbdParams {
+  float dt; /* frame dt; a substep uses dt / substeps */
+  int iterations;
+  float gravity[3];
+  float alpha, beta, gamma;
+  int post_stabilize;
+  float max_linear_speed, max_angular_speed;
+  int substeps;
+  float friction_static_mult;
+  int coloring_mode;         /* 0 = jacobi (speculative), 1 = jones_plassmann */
+  int recolor_every_substep; /* 1 = recolor every substep, 0 = on conflict */
+  int self_collide;
+  float self_friction;
+  int group_size;      /* lanes per body in the primal: 1,2,4,8,16,32 */
+  int use_graph;       /* capture one substep as a CUDA graph and replay it */
+  int persistent;      /* 1 = one cooperative kernel per substep solve */
+  int record_violation;/* store the max constraint violation per iteration */
+  int mlp_warm_start;  /* 1 = learned warm start for new contacts */
+  int debug_skip_arrive; /* test hook: block 0 skips one barrier arrival */
+  int blocks_per_sm;   /* persistent grid: CTAs per SM (0 = occupancy max) */
+} AvbdParams;
+
+typedef struct AvbdStats {
+  int n_pairs_found, n_pairs, n_dyn_groups, n_dyn_rows, n_dyn_rows_req;
+  int n_contacts_req, n_colors, recolored, conflicts, err, err_where;
+  int n_cache_hits, n_new_contacts, max_dg, n_viol;
+  unsigned epoch;
+  int graph_state;  /* bit 0: collision graph live, bit 1: solve graph live */
+  int capture_err;  /* 1000 * collision capture error + solve capture error */
+  long long kernels_launched; /* kernels enqueued by this context so far */
+  float viol[64];
+} AvbdStats;
+
+typedef struct AvbdCtx AvbdCtx;
+
+/* Arena layout.  `offsets` receives avbd_num_arrays() byte offsets. */
+int avbd_num_arrays(void);
+const char* avbd_array_name(int id);
+int avbd_layout(const AvbdDims* dims, size_t* offsets, size_t* total_bytes);
+
+/* Replaces Solver6DOF._flush's device allocation (solver_6dof.py:904-1174):
+ * binds a filled arena.  */
+int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx** out);
+int avbd_destroy(AvbdCtx* ctx);
+
+/* Scalars; no recapture is needed when they change (they live on device). */
+int avbd_set_params(AvbdCtx* ctx, const AvbdParams* p, void* stream);
+
+/* Marks every body uncolored, empties the contact cache and zeroes counters
+ * (the fresh-flush state of solver_6dof.py:1010-1035, 1150-1156). */
+int avbd_reset_state(AvbdCtx* ctx, void* stream);
+
+/* Forces a recolor on the next substep (solver_6dof.py:605-624 sets
+ * _color_dirty when the coloring mode changes). */
+int avbd_mark_color_dirty(AvbdCtx* ctx, void* stream);
+
+/* One substep of `dt` (replaces _step_one, solver_6dof.py:1232-1464). */
+int avbd_substep(AvbdCtx* ctx, float dt, void* stream);
+
+/* One frame: params.substeps substeps of dt/substeps (Solver6DOF.step,
+ * solver_6dof.py:1178-1197). */
+int avbd_step(AvbdCtx* ctx, void* stream);
+
+/* Device counters of the last substep; synchronises `stream`. */
+int avbd_read_stats(AvbdCtx* ctx, AvbdStats* out, void* stream);
+
+/* Diagnostic: active two-body contact pairs whose bodies share a color
+ * (count_color_conflicts, solver_6dof.py:846-862).  Synchronises. */
+int avbd_count_color_conflicts(AvbdCtx* ctx, void* stream);
+
+/* Replaces the contact cache with n entries: abc = n x (a, b, ordinal)
+ * int32 and state = n x 8 floats (lambda n/t/b, penalty n/t/b, was_static
+ * t/b), both device pointers; the next substep's emission looks them up.
+ * The reference keeps this state in hash_keys/hash_state
+ * (solver_6dof.py:1150-1156, kernels_6dof.py:2923-2995). */
+int avbd_cache_load(AvbdCtx* ctx, int n, const int* abc, const float* state, void* stream);
+
+/* Clears the sticky device error bits. */
+int avbd_clear_errors(AvbdCtx* ctx, void* stream);
+
+/* Device time of the last substep's collision and solve parts, in ms
+ * (replaces broadphase_ms, solver_6dof.py:1786-1787, 1916).  Synchronises. */
+int avbd_step_ms(AvbdCtx* ctx, float* collide_ms, float* solve_ms);
+
+/* Last error text of this thread. */
+const char* avbd_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AVBD6_H */
