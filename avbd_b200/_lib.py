@@ -31,7 +31,7 @@ class AvbdParams(C.Structure):
                 ("recolor_every_substep", C.c_int), ("self_collide", C.c_int), ("self_friction", C.c_float),
                 ("group_size", C.c_int), ("use_graph", C.c_int), ("persistent", C.c_int),
                 ("record_violation", C.c_int), ("mlp_warm_start", C.c_int), ("debug_skip_arrive", C.c_int),
-                ("blocks_per_sm", C.c_int)]
+                ("blocks_per_sm", C.c_int), ("timing", C.c_int)]
 
 
 class AvbdStats(C.Structure):
@@ -72,9 +72,11 @@ def load():
     L.avbd_cache_load.argtypes = [vp, i, vp, vp, vp]
     L.avbd_clear_errors.argtypes = [vp, vp]
     L.avbd_step_ms.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.avbd_read_phase_marks.argtypes = [vp, vp, vp, i, vp]
     for name in ("avbd_layout", "avbd_create", "avbd_destroy", "avbd_set_params", "avbd_reset_state",
                  "avbd_mark_color_dirty", "avbd_substep", "avbd_step", "avbd_read_stats",
-                 "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors", "avbd_step_ms"):
+                 "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors", "avbd_step_ms",
+                 "avbd_read_phase_marks"):
         getattr(L, name).restype = i
     _lib = L
     return L
@@ -91,4 +93,7 @@ def check(code: int, what: str) -> int:
 EXPORTED = ["avbd_num_arrays", "avbd_array_name", "avbd_layout", "avbd_create", "avbd_destroy",
             "avbd_set_params", "avbd_reset_state", "avbd_mark_color_dirty", "avbd_substep", "avbd_step",
             "avbd_read_stats", "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors",
-            "avbd_step_ms", "avbd_last_error"]
+            "avbd_step_ms", "avbd_read_phase_marks", "avbd_last_error"]
+
+PHASES = ["start", "gate+prelude", "color reset", "color rounds", "bucket", "predict", "primal", "dual",
+          "collect"]

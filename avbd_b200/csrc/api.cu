@@ -41,8 +41,8 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(PAIR_START, 4, N + 1) X(PAIR_AB, 8, P) X(PAIR_INFO, 4, P) X(PAIR_NRM, 16, P) X(PAIR_OFF, 16, 8 * P)        \
   X(PAIR_GCNT, 4, P) X(PAIR_GSTART, 4, P + 1) X(PAIR_RSTART, 4, P + 1) X(PAIR_KEPT, 4, P + 1) X(H_KEY, 8, H)   \
   X(H_S0, 16, H) X(H_S1, 16, H) X(SCAN_PART, 4, SP) X(SORT_HIST, 4, SH) X(C_USED, 4, N) X(C_LOST, 4, N)        \
-  X(C_HIST, 4, 64 * 32) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
-  X(COUNTERS, 1, (long long)sizeof(DevCounters))
+  X(C_HIST, 4, 64 * 64) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
+  X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,
@@ -95,7 +95,7 @@ struct AvbdCtx {
   size_t bytes;
   int num_sms;
   int coll_grid;
-  int solve_grid, solve_block;
+  int solve_grid, solve_block, solve_variant;
   cudaGraphExec_t exec[2];
   cudaGraph_t graph[2];
   bool graph_ok[2];
@@ -181,7 +181,7 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.node_right = PTR(int*, NODE_RIGHT); d.node_parent = PTR(int*, NODE_PARENT); d.node_flag = PTR(int*, NODE_FLAG);
   d.bounds = PTR(float*, BOUNDS);
   d.nbr_cnt = d.nbr_start = d.nbr_idx = d.nbr_pair = nullptr;
-  d.up_cnt = PTR(int*, UP_CNT); d.pair_start = PTR(int*, PAIR_START);
+  d.up_cnt = PTR(int*, UP_CNT); d.pair_start = PTR(int*, PAIR_START); d.bp_tmp = PTR(int*, BP_TMP);
   d.pair_ab = PTR(int2*, PAIR_AB); d.pair_info = PTR(int*, PAIR_INFO); d.pair_nrm = PTR(float4*, PAIR_NRM);
   d.pair_off = PTR(float4*, PAIR_OFF); d.pair_gcnt = PTR(int*, PAIR_GCNT); d.pair_gstart = PTR(int*, PAIR_GSTART);
   d.pair_rstart = PTR(int*, PAIR_RSTART); d.pair_kept = PTR(int*, PAIR_KEPT);
@@ -191,8 +191,9 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.mlp_w = dims->mlp_floats > 0 ? PTR(const float*, MLP_W) : nullptr;
   d.ctr = PTR(DevCounters*, COUNTERS);
 #undef PTR
-  int occ = solve_occupancy(256);
+  int occ = solve_occupancy(256, 2);
   c->solve_block = 256;
+  c->solve_variant = 2;
   c->solve_grid = c->num_sms * (occ > 0 ? occ : 1);
   c->P.dt = 1.0f / 60.0f;
   c->P.iterations = 10;
@@ -243,6 +244,7 @@ static void fill_devparams(AvbdCtx* c, float dt_sub) {
   q.debug_skip_arrive = P.debug_skip_arrive;
   q.mlp_on = P.mlp_warm_start && c->dims.mlp_floats > 0;
   q.barrier_timeout_ns = P.debug_skip_arrive ? 200000000ull : 2000000000ull;
+  q.timing = P.timing;
 }
 
 int avbd_set_params(AvbdCtx* c, const AvbdParams* p, void* stream) {
@@ -253,12 +255,13 @@ int avbd_set_params(AvbdCtx* c, const AvbdParams* p, void* stream) {
   fill_devparams(c, c->cur_dt);
   cudaError_t e = cudaMemcpyAsync((void*)c->d.prm, &c->dp, sizeof(DevParams), cudaMemcpyHostToDevice, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(AVBD_E_CUDA, "params upload", e);
-  if (p->blocks_per_sm > 0) {
-    int occ = solve_occupancy(256);
-    int b = p->blocks_per_sm < occ ? p->blocks_per_sm : occ;
-    int ng = c->num_sms * (b > 0 ? b : 1);
-    if (ng != c->solve_grid) c->solve_grid = ng;
-  }
+  // Persistent grid: `blocks_per_sm` CTAs per SM (0 = 2), using the
+  // register budget built for it, capped by the measured occupancy.
+  int want = p->blocks_per_sm > 0 ? p->blocks_per_sm : 2;
+  c->solve_variant = want >= 3 ? 3 : 2;
+  int occ = solve_occupancy(256, c->solve_variant);
+  int b = want < occ ? want : occ;
+  c->solve_grid = c->num_sms * (b > 0 ? b : 1);
   return AVBD_OK;
 }
 
@@ -286,7 +289,7 @@ static cudaError_t enqueue_part(AvbdCtx* c, int part, cudaStream_t st) {
     launch_collision(c->d, c->P, c->dims, c->coll_grid, st);
     e = cudaGetLastError();
   } else {
-    e = launch_solve(c->d, c->P, c->P.persistent, c->solve_grid, c->solve_block, st);
+    e = launch_solve(c->d, c->P, c->P.persistent, c->solve_grid, c->solve_block, st, c->solve_variant);
   }
   c->part_kernels[part] = (int)(g_kernel_launches - before);
   return e;
@@ -296,7 +299,7 @@ static void part_key(AvbdCtx* c, int part, int key[4]) {
   if (part == 0) {
     key[0] = c->P.self_collide; key[1] = c->coll_grid; key[2] = 0; key[3] = 0;
   } else {
-    key[0] = c->P.persistent; key[1] = c->solve_grid;
+    key[0] = c->P.persistent + 10 * c->solve_variant; key[1] = c->solve_grid;
     key[2] = c->P.persistent ? 0 : c->P.iterations + 100 * c->P.post_stabilize;
     key[3] = c->P.persistent ? 0 : c->P.coloring_mode;
   }
@@ -451,6 +454,22 @@ int avbd_step_ms(AvbdCtx* c, float* collide_ms, float* solve_ms) {
   if (collide_ms) *collide_ms = a;
   if (solve_ms) *solve_ms = b;
   return AVBD_OK;
+}
+
+int avbd_read_phase_marks(AvbdCtx* c, long long* t_ns, int* phase, int cap, void* stream) {
+  if (!c || !t_ns || !phase || cap < 0) return fail(AVBD_E_INVALID, "bad arguments");
+  DevCounters h;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(&h, c->d.ctr, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(AVBD_E_CUDA, "marks readback", e);
+  int n = h.n_marks < cap ? h.n_marks : cap;
+  if (n > 256) n = 256;
+  for (int k = 0; k < n; ++k) {
+    t_ns[k] = (long long)h.mark_t[k];
+    phase[k] = h.mark_id[k];
+  }
+  return n;
 }
 
 int avbd_count_color_conflicts(AvbdCtx* c, void* stream) {

@@ -28,7 +28,7 @@ __device__ __forceinline__ float ord2f(int i) { return __int_as_float(i >= 0 ? i
 // ---------------------------------------------------------------------------
 // Substep start: reset counters and the scene bounds used for Morton codes.
 // ---------------------------------------------------------------------------
-__global__ void k_begin_substep(Dev d) {
+__global__ void k_begin_substep(const __grid_constant__ Dev d) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     DevCounters* c = d.ctr;
     c->n_pairs_found = 0;
@@ -44,6 +44,7 @@ __global__ void k_begin_substep(Dev d) {
     c->max_dg = 0;
     c->n_viol = 0;
     c->bar_count = 0;
+    for (int k = 0; k < BAR_SUB; ++k) c->bar_sub[k][0] = 0;
     for (int k = 0; k < 64; ++k) c->viol_bits[k] = 0;
     int* b = (int*)d.bounds;
     b[0] = b[1] = b[2] = 0x7fffffff;
@@ -56,7 +57,7 @@ __global__ void k_begin_substep(Dev d) {
 
 // OBB -> world AABB with margin (kernels_6dof.py:1922-1943), plus the bounds
 // of the AABB centres for the Morton grid.
-__global__ void k_aabb(Dev d) {
+__global__ void k_aabb(const __grid_constant__ Dev d) {
   __shared__ int sb[6];
   if (threadIdx.x < 6) sb[threadIdx.x] = threadIdx.x < 3 ? 0x7fffffff : (int)0x80000000;
   __syncthreads();
@@ -89,7 +90,7 @@ __device__ __forceinline__ unsigned spread10(unsigned v) {
   return v;
 }
 
-__global__ void k_morton(Dev d) {
+__global__ void k_morton(const __grid_constant__ Dev d) {
   const int* b = (const int*)d.bounds;
   float lx = ord2f(b[0]), ly = ord2f(b[1]), lz = ord2f(b[2]);
   float hx = ord2f(b[3]), hy = ord2f(b[4]), hz = ord2f(b[5]);
@@ -296,7 +297,7 @@ __device__ __forceinline__ int delta(const unsigned* m, int n, int i, int j) {
   return __clz(a ^ b);
 }
 
-__global__ void k_lbvh_build(Dev d) {
+__global__ void k_lbvh_build(const __grid_constant__ Dev d) {
   int n = d.nb;
   const unsigned* m = d.morton;
   GSTRIDE(i, n - 1) {
@@ -335,7 +336,7 @@ __global__ void k_lbvh_build(Dev d) {
   if (blockIdx.x == 0 && threadIdx.x == 0) d.node_parent[0] = -1;
 }
 
-__global__ void k_lbvh_refit(Dev d) {
+__global__ void k_lbvh_refit(const __grid_constant__ Dev d) {
   int n = d.nb;
   GSTRIDE(k, n) {
     int node = n - 1 + k;
@@ -388,36 +389,60 @@ __device__ __forceinline__ void bvh_query_upper(const Dev& d, int i, F fn) {
   }
 }
 
-__global__ void k_bp_count(Dev d) {
-  GSTRIDE(i, d.nb) {
+// One traversal per body, threads in Morton order (a warp walks nearby
+// bodies, so its traversals share tree nodes).  The first BP_SLOTS upper
+// neighbours are kept in a per-body buffer for k_bp_fill.
+__global__ void k_bp_count(const __grid_constant__ Dev d) {
+  GSTRIDE(k, d.nb) {
+    int i = d.order[k];
     int c = 0;
-    bvh_query_upper(d, i, [&](int) { ++c; });
+    int* slot = d.bp_tmp + (size_t)i * BP_SLOTS;
+    bvh_query_upper(d, i, [&](int j) {
+      if (c < BP_SLOTS) slot[c] = j;
+      ++c;
+    });
     d.up_cnt[i] = c;
   }
 }
 
 // Writes body i's upper neighbours (j > i) as canonical pairs at
-// pair_start[i].., keeps those below pair_cap, and sorts them by j, so the
-// pair list is ordered by (i, j).
-__global__ void k_bp_fill(Dev d) {
+// pair_start[i].., sorted by j, keeping those below pair_cap, so the pair
+// list is ordered by (i, j).  Bodies with more than BP_SLOTS upper neighbours
+// traverse again.
+__global__ void k_bp_fill(const __grid_constant__ Dev d) {
   int cap = d.pair_cap;
-  GSTRIDE(i, d.nb) {
+  GSTRIDE(k, d.nb) {
+    int i = d.order[k];
     int s = d.pair_start[i];
-    int c = 0;
-    bvh_query_upper(d, i, [&](int j) {
-      int p = s + c;
-      if (p < cap) d.pair_ab[p] = make_int2(i, j);
-      ++c;
-    });
-    int e = min(s + c, cap);
-    for (int a = s + 1; a < e; ++a) {  // insertion sort by j
-      int2 v = d.pair_ab[a];
-      int b = a - 1;
-      while (b >= s && d.pair_ab[b].y > v.y) {
-        d.pair_ab[b + 1] = d.pair_ab[b];
-        --b;
+    int n = d.up_cnt[i];
+    if (s >= cap || n == 0) continue;
+    if (n <= BP_SLOTS) {
+      int v[BP_SLOTS];
+      const int* slot = d.bp_tmp + (size_t)i * BP_SLOTS;
+      for (int a = 0; a < n; ++a) {  // insertion sort by j
+        int x = slot[a];
+        int b = a - 1;
+        while (b >= 0 && v[b] > x) {
+          v[b + 1] = v[b];
+          --b;
+        }
+        v[b + 1] = x;
       }
-      d.pair_ab[b + 1] = v;
+      int e = min(n, cap - s);
+      for (int a = 0; a < e; ++a) d.pair_ab[s + a] = make_int2(i, v[a]);
+      continue;
+    }
+    // Rare: more neighbours than slots.  Keep the smallest j's below the cap
+    // by repeated selection over fresh traversals (bounded by n).
+    int e = min(n, cap - s);
+    int last = -1;
+    for (int a = 0; a < e; ++a) {
+      int best = 0x7fffffff;
+      bvh_query_upper(d, i, [&](int j) {
+        if (j > last && j < best) best = j;
+      });
+      d.pair_ab[s + a] = make_int2(i, best);
+      last = best;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -653,7 +678,7 @@ __device__ void sat_manifold(V3 cA, M3 RA, V3 eA, V3 cB, M3 RB, V3 eB, Manifold&
 }
 
 // SAT + manifold per pair; writes the per-pair group/row counts for the scans.
-__global__ void k_narrow(Dev d) {
+__global__ void k_narrow(const __grid_constant__ Dev d) {
   int np = d.ctr->n_pairs;
   float self_friction = d.prm->self_friction;
   GSTRIDE(p, np) {
@@ -697,7 +722,7 @@ __device__ __forceinline__ int cache_find(const Dev& d, unsigned long long k, un
 // numbered after the static rows in pair order; contacts whose rows would
 // pass the dynamic row capacity are dropped (:2795-2800).  Warm start from
 // the contact cache, else lambda = 0, k = (1e6, 1, 1).
-__global__ void k_emit(Dev d, int dyn_row_cap, int dyn_group_cap) {
+__global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_group_cap) {
   int np = d.ctr->n_pairs;
   float self_friction = d.prm->self_friction, fsm = d.prm->fsm;
   unsigned tag = epoch_tag(d.ctr->epoch);
@@ -763,7 +788,7 @@ __global__ void k_emit(Dev d, int dyn_row_cap, int dyn_group_cap) {
 
 // Per-body dynamic incidence lists (group ids), then sorted ascending so the
 // primal's summation order is reproducible.
-__global__ void k_dg_fill(Dev d) {
+__global__ void k_dg_fill(const __grid_constant__ Dev d) {
   int np = d.ctr->n_pairs;
   GSTRIDE(p, np) {
     int kept = d.pair_kept[p];
@@ -779,11 +804,11 @@ __global__ void k_dg_fill(Dev d) {
   }
 }
 
-__global__ void k_dg_zero(Dev d) {
+__global__ void k_dg_zero(const __grid_constant__ Dev d) {
   GSTRIDE(i, d.nb) d.dg_cnt[i] = 0;
 }
 
-__global__ void k_dg_sort(Dev d) {
+__global__ void k_dg_sort(const __grid_constant__ Dev d) {
   GSTRIDE(i, d.nb) {
     int s = d.dg_start[i], e = d.dg_start[i + 1];
     for (int a = s + 1; a < e; ++a) {
@@ -800,7 +825,7 @@ __global__ void k_dg_sort(Dev d) {
 }
 
 // Empties dynamic incidence lists when self collision is off (static-only scenes).
-__global__ void k_dg_clear(Dev d) {
+__global__ void k_dg_clear(const __grid_constant__ Dev d) {
   GSTRIDE(i, d.nb + 1) d.dg_start[i] = 0;
 }
 

@@ -29,8 +29,9 @@ __host__ __device__ inline int make_meta(int kind, int three, int hard, int cidx
   return kind | (three ? 4 : 0) | (hard ? 8 : 0) | (cidx << 4);
 }
 // g_flags bit layout: bits 0-2 row active, bit 3 normal row was_static,
-// bits 4/5 the friction rows' own was_static (carried to the cache).
-enum : int { FL_ACT0 = 1, FL_ACT1 = 2, FL_ACT2 = 4, FL_WAS = 8, FL_WAST = 16, FL_WASB = 32 };
+// bits 4/5 the friction rows' own was_static (carried to the cache), bit 6:
+// body_b owns the group (runs its dual update; else body_a).
+enum : int { FL_ACT0 = 1, FL_ACT1 = 2, FL_ACT2 = 4, FL_WAS = 8, FL_WAST = 16, FL_WASB = 32, FL_OWNB = 64 };
 
 // Penalty constants: kernels_6dof.py:50-52.
 #define PEN_MIN 1.0e6f
@@ -39,6 +40,7 @@ enum : int { FL_ACT0 = 1, FL_ACT1 = 2, FL_ACT2 = 4, FL_WAS = 8, FL_WAST = 16, FL
 #define MAX_COLORS 32
 #define JP_ROUNDS 24
 #define COLL_MARGIN 0.005f
+#define BP_SLOTS 32
 
 // Error bits of the device status word.
 enum : int {
@@ -73,13 +75,22 @@ struct DevCounters {
   int max_dg;            // longest per-body dynamic incidence list
   unsigned viol_bits[64];  // per-iteration max violation (float bits, >= 0)
   int n_viol;
-  int pad[15];
-  // grid barrier state (kept on its own 128-byte lines)
+  int n_marks;           // phase timestamps recorded (timing mode)
+  int pad[14];
+  unsigned long long mark_t[256];  // globaltimer after each grid barrier
+  int mark_id[256];                // phase id of that barrier (PH_*)
+  // grid barrier state (each counter on its own 128-byte line): blocks
+  // arrive on one of BAR_SUB sub-counters; the last of each sub-group
+  // arrives on the top counter; the last of those bumps the generation.
   unsigned bar_count;
   unsigned pad2[31];
   unsigned bar_gen;
   unsigned pad3[31];
+  unsigned bar_sub[16][32];
+  int round_unc[2];  // uncolored counts of alternate coloring rounds
+  int pad4[30];
 };
+#define BAR_SUB 16
 
 // Scalars read by the kernels from device memory, so a captured graph sees
 // parameter changes without being re-captured.
@@ -99,7 +110,14 @@ struct DevParams {
   int debug_skip_arrive;
   int mlp_on;
   unsigned long long barrier_timeout_ns;
-  int pad[8];
+  int timing;  // record phase timestamps in the counters
+  int pad[7];
+};
+
+// Phase ids of the persistent kernel's timestamps.
+enum : int {
+  PH_START = 0, PH_GATE_PRELUDE, PH_COLOR_RESET, PH_ROUND, PH_BUCKET, PH_PREDICT, PH_PRIMAL, PH_DUAL, PH_COLLECT,
+  PH_COUNT
 };
 
 // Every device pointer and size one substep needs.  Passed by value.
@@ -127,6 +145,7 @@ struct Dev {
   float* bounds;  // 6 floats (lo xyz, hi xyz) as ordered ints
   int *nbr_cnt, *nbr_start, *nbr_idx, *nbr_pair;
   int *up_cnt, *pair_start;
+  int* bp_tmp;  // BP_SLOTS upper neighbours per body from the traversal
   int2* pair_ab;
   int* pair_info;     // overlap | sat_idx<<1 | count<<6 | ref_is_a<<9
   float4* pair_nrm;   // manifold normal (inc -> ref), w = SAT depth

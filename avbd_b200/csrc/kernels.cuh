@@ -15,8 +15,11 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
 
 // Solve: coloring + predict + prelude + iterations + cache refresh.
 // persistent = one cooperative launch; otherwise one launch per phase.
-cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st);
-int solve_occupancy(int block);  // resident CTAs per SM of the persistent kernel
+cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st,
+                         int variant);
+// Resident CTAs per SM of the persistent kernel built for `variant` (2 or 3)
+// CTAs per SM.
+int solve_occupancy(int block, int variant);
 void launch_reset(Dev& d, cudaStream_t st);
 int count_conflicts(Dev& d, cudaStream_t st);
 void launch_hash_scrub(Dev& d, cudaStream_t st);

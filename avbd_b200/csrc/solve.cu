@@ -49,28 +49,43 @@ __device__ bool grid_barrier(const Dev& d, int idx) {
       bool skip = d.prm->debug_skip_arrive && blockIdx.x == 0 && idx == 0;
       bool last = false;
       if (!skip) {
-        unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
-        if (arrived == gridDim.x - 1) {
-          cnt.store(0u, cuda::memory_order_relaxed);
-          gen.fetch_add(1u, cuda::memory_order_release);
-          last = true;
+        // Two-level arrival: BAR_SUB sub-counters keep the serialized atomics
+        // per address at about gridDim / BAR_SUB.
+        unsigned nblk = gridDim.x;
+        unsigned nsub = nblk < BAR_SUB ? nblk : BAR_SUB;
+        unsigned sub = blockIdx.x % nsub;
+        unsigned members = nblk / nsub + (sub < nblk % nsub ? 1u : 0u);
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> sc(c->bar_sub[sub][0]);
+        unsigned a_sub = sc.fetch_add(1u, cuda::memory_order_acq_rel);
+        if (a_sub == members - 1) {
+          sc.store(0u, cuda::memory_order_relaxed);
+          unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+          if (arrived == nsub - 1) {
+            cnt.store(0u, cuda::memory_order_relaxed);
+            gen.fetch_add(1u, cuda::memory_order_release);
+            last = true;
+          }
         }
       }
       if (!last) {
+        // Poll the generation word; the timer and the abort flag are checked
+        // every 64 polls so a healthy wait costs one L2 round trip per poll.
         unsigned long long t0 = gtimer();
         unsigned long long budget = d.prm->barrier_timeout_ns;
+        unsigned spins = 0;
         while (gen.load(cuda::memory_order_acquire) == g) {
-          if (err.load(cuda::memory_order_relaxed) & ERR_BARRIER_TIMEOUT) {
-            ok = 0;
-            break;
+          if ((++spins & 63u) == 0u) {
+            if (err.load(cuda::memory_order_relaxed) & ERR_BARRIER_TIMEOUT) {
+              ok = 0;
+              break;
+            }
+            if (gtimer() - t0 > budget) {
+              err.fetch_or(ERR_BARRIER_TIMEOUT, cuda::memory_order_relaxed);
+              atomicMax(&c->err_where, idx);
+              ok = 0;
+              break;
+            }
           }
-          if (gtimer() - t0 > budget) {
-            err.fetch_or(ERR_BARRIER_TIMEOUT, cuda::memory_order_relaxed);
-            atomicMax(&c->err_where, idx);
-            ok = 0;
-            break;
-          }
-          __nanosleep(40);
         }
       }
       __threadfence();
@@ -162,52 +177,93 @@ __device__ __forceinline__ void acc_axis(Acc& s, V3 rs, float f, float kl) {
   s.ra[0] += ja.x * f; s.ra[1] += ja.y * f; s.ra[2] += ja.z * f;
 }
 
-// Contribution of group g to body i's system (rows in row order).
-__device__ __forceinline__ void accumulate_group(const Dev& d, int g, int i, V3 xi, float4 qi, bool post, Acc& s) {
+// Dual update of one group's rows in row order (kernels_6dof.py:1451-1548):
+// a friction row sees its normal row's new lambda and was_static flag.
+// Craw are the rows' constraint values at the current pose; ac the stored
+// alpha*C0.  Returns the largest violation of the non-friction rows.
+__device__ __forceinline__ float dual_rows(int kind, int nr, bool hard, float4 mat, const float* Craw, const float* ac,
+                                           float beta, float* lm, float* pn, int& fl) {
+  bool tang = kind != KIND_PIN;
+  float vmax = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (k >= nr || !(fl & (1 << k))) continue;
+    float C = hard ? Craw[k] - ac[k] : Craw[k];
+    float le = hard ? lm[k] : 0.0f;
+    float lo, hi;
+    bool is_t = tang && k > 0;
+    bool used_static = false;
+    if (is_t) {
+      float mu = mat.x;
+      if (fl & FL_WAS) {
+        mu = mat.y;
+        used_static = true;
+      }
+      float bound = mu * fabsf(lm[0]);
+      lo = -bound;
+      hi = bound;
+    } else {
+      lo = -FINF;
+      hi = kind == KIND_PIN ? FINF : 0.0f;
+      vmax = fmaxf(vmax, kind == KIND_PIN ? fabsf(Craw[k]) : fmaxf(0.0f, -Craw[k]));
+    }
+    float nl = fminf(fmaxf(pn[k] * C + le, lo), hi);
+    lm[k] = nl;
+    if (fabsf(nl) >= mat.w) {  // fracture
+      fl &= ~(1 << k);
+      lm[k] = 0.0f;
+      pn[k] = 0.0f;
+      continue;
+    }
+    if (nl > lo && nl < hi) {
+      pn[k] = fminf(pn[k] + beta * fabsf(C), fminf(PEN_MAX, mat.z));
+    } else if (is_t && used_static) {
+      fl &= ~FL_WAS;  // static -> dynamic friction (AVBD sec. 3.3)
+    }
+  }
+  return vmax;
+}
+
+// Group g's contribution to body i's system, rows in row order.  When
+// `dual` is set and body i owns g (the group's dynamic body with the lower
+// color), the previous iteration's dual update of g is applied first: both
+// bodies still hold their poses from the end of that iteration, because the
+// owner's color runs before the other body's.  Returns the violation of the
+// updated rows (0 when no dual ran).
+__device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3 xi, float4 qi, bool post, bool dual,
+                                                  Acc& s) {
   int meta = d.g_meta[g];
   int fl = d.g_flags[g];
   int kind = meta_kind(meta);
   bool three = (meta & 4) != 0, hard = (meta & 8) != 0;
-  float4 lam = d.g_lam[g], pen = d.g_pen[g], ac0 = d.g_ac0[g];
-  if (post) {  // post-stabilization pass: alpha = 0 for non-friction rows (kernels_6dof.py:1733-1811)
-    ac0.x = 0.0f;
-    if (kind == KIND_PIN) { ac0.y = 0.0f; ac0.z = 0.0f; }
-  }
-  float f, kl;
+  int nr = three ? 3 : 1;
+  float4 lam = d.g_lam[g], pen = d.g_pen[g], ac0 = d.g_ac0[g], mat = d.g_mat[g];
+  float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z}, ac[3] = {ac0.x, ac0.y, ac0.z};
+  float C[3] = {0.0f, 0.0f, 0.0f};
+  V3 rs, dirs[3], dd;
+  float sg = 1.0f;
+  bool own = true;
   if (kind == KIND_FLOOR) {
     float4 oa = d.g_offa[g];
-    V3 rs = qrot(qi, xyz(oa));
-    if (fl & FL_ACT0) {
-      row_force((xi.y + rs.y) - oa.w, hard, ac0.x, lam.x, pen.x, -FINF, 0.0f, f, kl);
-      acc_axis<1>(s, rs, f, kl);
-    }
-    if (three) {
-      float4 mat = d.g_mat[g];
-      float bound = ((fl & FL_WAS) ? mat.y : mat.x) * fabsf(lam.x);
-      if (fl & FL_ACT1) {
-        row_force(xi.x + rs.x, hard, ac0.y, lam.y, pen.y, -bound, bound, f, kl);
-        acc_axis<0>(s, rs, f, kl);
-      }
-      if (fl & FL_ACT2) {
-        row_force(xi.z + rs.z, hard, ac0.z, lam.z, pen.z, -bound, bound, f, kl);
-        acc_axis<2>(s, rs, f, kl);
-      }
-    }
+    rs = qrot(qi, xyz(oa));
+    C[0] = (xi.y + rs.y) - oa.w;
+    C[1] = xi.x + rs.x;  // dot((1,0,0), x + R off)
+    C[2] = xi.z + rs.z;  // dot((0,0,1), x + R off)
   } else if (kind == KIND_PIN) {
     float4 oa = d.g_offa[g], an = d.g_n[g];
-    V3 rs = qrot(qi, xyz(oa));
+    rs = qrot(qi, xyz(oa));
     V3 p = xi + rs;
-    if (fl & FL_ACT0) { row_force(p.x - an.x, hard, ac0.x, lam.x, pen.x, -FINF, FINF, f, kl); acc_axis<0>(s, rs, f, kl); }
-    if (fl & FL_ACT1) { row_force(p.y - an.y, hard, ac0.y, lam.y, pen.y, -FINF, FINF, f, kl); acc_axis<1>(s, rs, f, kl); }
-    if (fl & FL_ACT2) { row_force(p.z - an.z, hard, ac0.z, lam.z, pen.z, -FINF, FINF, f, kl); acc_axis<2>(s, rs, f, kl); }
+    C[0] = p.x - an.x;
+    C[1] = p.y - an.y;
+    C[2] = p.z - an.z;
   } else {
     int2 bd = d.g_body[g];
     bool side_a = bd.x == i;
+    own = ((fl & FL_OWNB) != 0) == !side_a;
     int o = side_a ? bd.y : bd.x;
     float4 xo4 = d.x[o], qo = d.q[o];
     float4 oa = d.g_offa[g], ob = d.g_offb[g];
     V3 n = xyz(d.g_n[g]);
-    V3 rs, dd;
     if (side_a) {
       rs = qrot(qi, xyz(oa));
       V3 ro = qrot(qo, xyz(ob));
@@ -217,26 +273,63 @@ __device__ __forceinline__ void accumulate_group(const Dev& d, int g, int i, V3 
       rs = qrot(qi, xyz(ob));
       dd = (xyz(xo4) + ro) - (xi + rs);
     }
-    float sg = side_a ? 1.0f : -1.0f;
+    sg = side_a ? 1.0f : -1.0f;
+    dirs[0] = n;
+    C[0] = dot(n, dd);
+    if (three) {
+      dirs[1] = orthonormal_basis(n);
+      dirs[2] = cross(n, dirs[1]);
+      C[1] = dot(dirs[1], dd);
+      C[2] = dot(dirs[2], dd);
+    }
+  }
+  float viol = 0.0f;
+  if (dual && own) {
+    viol = dual_rows(kind, nr, hard, mat, C, ac, d.prm->beta, lm, pn, fl);
+    d.g_lam[g] = make_float4(lm[0], lm[1], lm[2], 0.0f);
+    d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
+    d.g_flags[g] = fl;
+  }
+  if (post) {  // post-stabilization pass: alpha = 0 for non-friction rows (kernels_6dof.py:1733-1811)
+    ac[0] = 0.0f;
+    if (kind == KIND_PIN) ac[1] = ac[2] = 0.0f;
+  }
+  float f, kl;
+  if (kind == KIND_FLOOR) {
     if (fl & FL_ACT0) {
-      row_force(dot(n, dd), hard, ac0.x, lam.x, pen.x, -FINF, 0.0f, f, kl);
-      acc_row(s, n * sg, cross(rs, n) * sg, n, rs, f, kl);
+      row_force(C[0], hard, ac[0], lm[0], pn[0], -FINF, 0.0f, f, kl);
+      acc_axis<1>(s, rs, f, kl);
     }
     if (three) {
-      float4 mat = d.g_mat[g];
-      float bound = ((fl & FL_WAS) ? mat.y : mat.x) * fabsf(lam.x);
-      V3 t = orthonormal_basis(n);
-      V3 b = cross(n, t);
+      float bound = ((fl & FL_WAS) ? mat.y : mat.x) * fabsf(lm[0]);
       if (fl & FL_ACT1) {
-        row_force(dot(t, dd), hard, ac0.y, lam.y, pen.y, -bound, bound, f, kl);
-        acc_row(s, t * sg, cross(rs, t) * sg, t, rs, f, kl);
+        row_force(C[1], hard, ac[1], lm[1], pn[1], -bound, bound, f, kl);
+        acc_axis<0>(s, rs, f, kl);
       }
       if (fl & FL_ACT2) {
-        row_force(dot(b, dd), hard, ac0.z, lam.z, pen.z, -bound, bound, f, kl);
-        acc_row(s, b * sg, cross(rs, b) * sg, b, rs, f, kl);
+        row_force(C[2], hard, ac[2], lm[2], pn[2], -bound, bound, f, kl);
+        acc_axis<2>(s, rs, f, kl);
+      }
+    }
+  } else if (kind == KIND_PIN) {
+    if (fl & FL_ACT0) { row_force(C[0], hard, ac[0], lm[0], pn[0], -FINF, FINF, f, kl); acc_axis<0>(s, rs, f, kl); }
+    if (fl & FL_ACT1) { row_force(C[1], hard, ac[1], lm[1], pn[1], -FINF, FINF, f, kl); acc_axis<1>(s, rs, f, kl); }
+    if (fl & FL_ACT2) { row_force(C[2], hard, ac[2], lm[2], pn[2], -FINF, FINF, f, kl); acc_axis<2>(s, rs, f, kl); }
+  } else {
+    if (fl & FL_ACT0) {
+      row_force(C[0], hard, ac[0], lm[0], pn[0], -FINF, 0.0f, f, kl);
+      acc_row(s, dirs[0] * sg, cross(rs, dirs[0]) * sg, dirs[0], rs, f, kl);
+    }
+    if (three) {
+      float bound = ((fl & FL_WAS) ? mat.y : mat.x) * fabsf(lm[0]);
+      for (int k = 1; k < 3; ++k) {
+        if (!(fl & (1 << k))) continue;
+        row_force(C[k], hard, ac[k], lm[k], pn[k], -bound, bound, f, kl);
+        acc_row(s, dirs[k] * sg, cross(rs, dirs[k]) * sg, dirs[k], rs, f, kl);
       }
     }
   }
+  return viol;
 }
 
 // 3x3 inverse by the adjugate (zero matrix when singular).
@@ -314,13 +407,61 @@ __device__ __forceinline__ void solve_body(const Dev& d, int i, float4 xi4, floa
   d.q[i] = nq;
 }
 
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// L1 prefetch of the SoA records group g's evaluation reads (static groups
+// are floor corners or pins; dynamic groups are box-box contacts).
+__device__ __forceinline__ void prefetch_group(const Dev& d, int g, bool box) {
+  prefetch_l1(d.g_meta + g);
+  prefetch_l1(d.g_flags + g);
+  prefetch_l1(d.g_lam + g);
+  prefetch_l1(d.g_pen + g);
+  prefetch_l1(d.g_ac0 + g);
+  prefetch_l1(d.g_mat + g);
+  prefetch_l1(d.g_offa + g);
+  if (box) {
+    prefetch_l1(d.g_body + g);
+    prefetch_l1(d.g_offb + g);
+    prefetch_l1(d.g_n + g);
+  }
+}
+
+// BDF1 velocities + caps of one body (kernels_6dof.py:1871-1901).
+__device__ __forceinline__ void finalize_body(const Dev& d, int i, float dt) {
+  const DevParams& P = *d.prm;
+  float4 v = d.v[i], w = d.w[i];
+  d.pv[i] = v;
+  d.pw[i] = w;
+  float4 x = d.x[i];
+  if (x.w > 0.0f) {
+    float4 x0 = d.x0[i];
+    V3 nv = V3{x.x - x0.x, x.y - x0.y, x.z - x0.z} / dt;
+    V3 nw = quat_to_rotvec(qmul(d.q[i], qconj(d.q0[i]))) / dt;
+    float sl = sqrtf(dot(nv, nv));
+    if (sl > P.max_lin) nv = nv * (P.max_lin / sl);
+    float sa = sqrtf(dot(nw, nw));
+    if (sa > P.max_ang) nw = nw * (P.max_ang / sa);
+    d.v[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+    d.w[i] = make_float4(nw.x, nw.y, nw.z, 0.0f);
+  }
+}
+
+// Which flags a color pass carries.
+struct PassMode {
+  bool post;      // post-stabilization primal (alpha = 0 for non-friction rows)
+  bool dual;      // apply the previous iteration's dual update (owned groups)
+  bool finalize;  // BDF1 finalize of the body before its primal
+  int viol_slot;  // iteration whose violation is recorded (-1: none)
+};
+
 // Primal sweep of one color: G lanes per body, butterfly reduction of the
 // 27 accumulators, lane 0 solves (kernels_6dof.py:1149-1414, in place).
 template <int G>
-__device__ void primal_color(const Dev& d, int c, bool post, float dt, int gtid, int gsize) {
+__device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gtid, int gsize) {
   int cs0 = d.color_starts[c];
   int nbody = d.color_starts[c + 1] - cs0;
   int total = nbody * G;
+  float vmax = 0.0f;
   for (int base = 0; base < total; base += gsize) {
     int t = base + gtid;
     int slot = t / G, lane = t & (G - 1);
@@ -328,6 +469,7 @@ __device__ void primal_color(const Dev& d, int c, bool post, float dt, int gtid,
     int i = valid ? d.color_bodies[cs0 + slot] : 0;
     float4 xi4 = valid ? d.x[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     bool act = valid && xi4.w > 0.0f;
+    if (pm.finalize && valid && lane == 0) finalize_body(d, i, dt);
     Acc s;
     acc_zero(s);
     float4 qi = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
@@ -336,9 +478,15 @@ __device__ void primal_color(const Dev& d, int c, bool post, float dt, int gtid,
       V3 xi = xyz(xi4);
       int s0 = d.sg_start[i], ns = d.sg_start[i + 1] - s0;
       int e0 = d.dg_start[i], nd = d.dg_start[i + 1] - e0;
+      // Issue every group record this lane will read before evaluating any,
+      // so the per-group dependent loads overlap instead of chaining.
+      for (int k = lane; k < ns + nd; k += G) {
+        if (k < ns) prefetch_group(d, s0 + k, false);
+        else prefetch_group(d, d.dg_idx[e0 + (k - ns)], true);
+      }
       for (int k = lane; k < ns + nd; k += G) {
         int g = k < ns ? s0 + k : d.dg_idx[e0 + (k - ns)];
-        accumulate_group(d, g, i, xi, qi, post, s);
+        vmax = fmaxf(vmax, accumulate_group(d, g, i, xi, qi, pm.post, pm.dual, s));
       }
     }
     if (G > 1) {
@@ -360,18 +508,33 @@ __device__ void primal_color(const Dev& d, int c, bool post, float dt, int gtid,
     }
     if (act && lane == 0) solve_body(d, i, xi4, qi, s, dt);
   }
+  if (pm.viol_slot >= 0) {
+    for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    if (lane_id() == 0 && vmax > 0.0f) atomicMax(&d.ctr->viol_bits[pm.viol_slot], __float_as_uint(vmax));
+  }
 }
 
-__device__ void ph_primal(const Dev& d, int c, bool post, int gtid, int gsize) {
+__device__ void ph_primal(const Dev& d, int c, PassMode pm, int gtid, int gsize) {
   float dt = d.prm->dt;
   switch (d.prm->group_size) {
-    case 1: primal_color<1>(d, c, post, dt, gtid, gsize); break;
-    case 2: primal_color<2>(d, c, post, dt, gtid, gsize); break;
-    case 4: primal_color<4>(d, c, post, dt, gtid, gsize); break;
-    case 8: primal_color<8>(d, c, post, dt, gtid, gsize); break;
-    case 16: primal_color<16>(d, c, post, dt, gtid, gsize); break;
-    default: primal_color<32>(d, c, post, dt, gtid, gsize); break;
+    case 1: primal_color<1>(d, c, pm, dt, gtid, gsize); break;
+    case 2: primal_color<2>(d, c, pm, dt, gtid, gsize); break;
+    case 4: primal_color<4>(d, c, pm, dt, gtid, gsize); break;
+    case 8: primal_color<8>(d, c, pm, dt, gtid, gsize); break;
+    case 16: primal_color<16>(d, c, pm, dt, gtid, gsize); break;
+    default: primal_color<32>(d, c, pm, dt, gtid, gsize); break;
   }
+}
+
+// Flags of iteration `it` of `total` (= iterations + post-stab pass).
+__device__ __forceinline__ PassMode pass_mode(const DevParams& P, int it) {
+  PassMode pm;
+  int iters = P.iterations;
+  pm.post = P.post_stab && it == iters;
+  pm.dual = it >= 1 && it <= iters;  // dual of iteration it-1
+  pm.finalize = P.post_stab && it == iters && iters >= 1;
+  pm.viol_slot = (P.record_violation && pm.dual && it - 1 < 64) ? it - 1 : -1;
+  return pm;
 }
 
 // ---------------------------------------------------------------------------
@@ -434,7 +597,9 @@ __device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
     bool tang = kind != KIND_PIN;  // rows 1, 2 of floor/box groups are friction rows
     float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z};
     int nr = three ? 3 : 1;
-    for (int k = 0; k < nr; ++k) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (k >= nr) break;
       float kf = (tang && k > 0) ? PEN_MIN_T : PEN_MIN;
       float p = fminf(fmaxf(pn[k] * P.gamma, kf), PEN_MAX);
       if (!P.post_stab) lm[k] = lm[k] * P.alpha * P.gamma;
@@ -453,8 +618,9 @@ __device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
     }
     GroupC c0 = group_values(d, g, meta, d.x, d.q);
     float a[3] = {0.0f, 0.0f, 0.0f};
-    for (int k = 0; k < nr; ++k) {
-      if (!(fl & (1 << k))) continue;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (k >= nr || !(fl & (1 << k))) continue;
       float C0 = c0.c[k];
       if (tang && k > 0) a[k] = C0;
       else if (kind != KIND_PIN) a[k] = C0 > 0.0f ? 0.0f : main_alpha * C0;
@@ -467,8 +633,9 @@ __device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
   }
 }
 
-// Dual update (kernels_6dof.py:1451-1548), rows of a group in row order.
-// Optionally records the max constraint violation of this iteration.
+// Stand-alone dual update of every group (kernels_6dof.py:1451-1548); used
+// after the last iteration when there is no post-stabilization pass to carry
+// it, and by the split path.  Optionally records the iteration's violation.
 __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
   const DevParams& P = *d.prm;
   int ng = n_groups_live(d);
@@ -482,43 +649,7 @@ __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
     float4 lam = d.g_lam[g], pen = d.g_pen[g], ac0 = d.g_ac0[g], mat = d.g_mat[g];
     GroupC cv = group_values(d, g, meta, d.x, d.q);
     float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z}, ac[3] = {ac0.x, ac0.y, ac0.z};
-    bool tang = kind != KIND_PIN;
-    int nr = three ? 3 : 1;
-    for (int k = 0; k < nr; ++k) {
-      if (!(fl & (1 << k))) continue;
-      float Craw = cv.c[k];
-      float C = hard ? Craw - ac[k] : Craw;
-      float le = hard ? lm[k] : 0.0f;
-      float lo, hi;
-      bool is_t = tang && k > 0;
-      bool used_static = false;
-      if (is_t) {
-        float mu = mat.x;
-        if (fl & FL_WAS) { mu = mat.y; used_static = true; }
-        float bound = mu * fabsf(lm[0]);
-        lo = -bound;
-        hi = bound;
-      } else {
-        lo = -FINF;
-        hi = kind == KIND_PIN ? FINF : 0.0f;
-        float v = kind == KIND_PIN ? fabsf(Craw) : fmaxf(0.0f, -Craw);
-        vmax = fmaxf(vmax, v);
-      }
-      float nl = fminf(fmaxf(pn[k] * C + le, lo), hi);
-      lm[k] = nl;
-      if (fabsf(nl) >= mat.w) {
-        fl &= ~(1 << k);
-        lm[k] = 0.0f;
-        pn[k] = 0.0f;
-        continue;
-      }
-      if (nl > lo && nl < hi) {
-        float up = fminf(PEN_MAX, mat.z);
-        pn[k] = fminf(pn[k] + P.beta * fabsf(C), up);
-      } else if (is_t && used_static) {
-        fl &= ~FL_WAS;
-      }
-    }
+    vmax = fmaxf(vmax, dual_rows(kind, three ? 3 : 1, hard, mat, cv.c, ac, P.beta, lm, pn, fl));
     d.g_lam[g] = make_float4(lm[0], lm[1], lm[2], 0.0f);
     d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
     d.g_flags[g] = fl;
@@ -529,7 +660,9 @@ __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
   }
 }
 
-// Inertial target + warm start (kernels_6dof.py:122-187).
+// Inertial target + warm start (kernels_6dof.py:122-187), plus the owner of
+// every contact group for the fused dual: its dynamic body with the lower
+// color (a static body never runs a primal, so it never owns).
 __device__ void ph_predict(const Dev& d, int gtid, int gsize) {
   const DevParams& P = *d.prm;
   float dt = P.dt;
@@ -571,29 +704,21 @@ __device__ void ph_predict(const Dev& d, int gtid, int gsize) {
     d.x[i] = make_float4(xw.x, xw.y, xw.z, m);
     d.q[i] = qn;
   }
+  int nd = d.ctr->n_dyn_groups;
+  for (int u = gtid; u < nd; u += gsize) {
+    int g = d.n_sg + u;
+    int2 bd = d.g_body[g];
+    bool sa = d.x[bd.x].w <= 0.0f, sb = d.x[bd.y].w <= 0.0f;  // mass in .w is never changed by predict
+    bool ownb = sa || (!sb && d.color[bd.y] < d.color[bd.x]);
+    int fl = d.g_flags[g];
+    d.g_flags[g] = ownb ? (fl | FL_OWNB) : (fl & ~FL_OWNB);
+  }
 }
 
-// BDF1 velocities + caps (kernels_6dof.py:1871-1901).
+// BDF1 velocities + caps of every body (kernels_6dof.py:1871-1901).
 __device__ void ph_finalize(const Dev& d, int gtid, int gsize) {
-  const DevParams& P = *d.prm;
-  float dt = P.dt;
-  for (int i = gtid; i < d.nb; i += gsize) {
-    float4 v = d.v[i], w = d.w[i];
-    d.pv[i] = v;
-    d.pw[i] = w;
-    float4 x = d.x[i];
-    if (x.w > 0.0f) {
-      float4 x0 = d.x0[i];
-      V3 nv = V3{x.x - x0.x, x.y - x0.y, x.z - x0.z} / dt;
-      V3 nw = quat_to_rotvec(qmul(d.q[i], qconj(d.q0[i]))) / dt;
-      float sl = sqrtf(dot(nv, nv));
-      if (sl > P.max_lin) nv = nv * (P.max_lin / sl);
-      float sa = sqrtf(dot(nw, nw));
-      if (sa > P.max_ang) nw = nw * (P.max_ang / sa);
-      d.v[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
-      d.w[i] = make_float4(nw.x, nw.y, nw.z, 0.0f);
-    }
-  }
+  float dt = d.prm->dt;
+  for (int i = gtid; i < d.nb; i += gsize) finalize_body(d, i, dt);
 }
 
 // Contact-cache refresh (kernels_6dof.py:2923-2995) with an epoch tag in
@@ -682,6 +807,7 @@ __device__ void ph_color_reset(const Dev& d, int gtid, int gsize) {
   }
   if (gtid == 0) {
     d.ctr->uncolored = 0;
+    d.ctr->round_unc[0] = 0;
     d.ctr->recolored = 1;
   }
 }
@@ -711,7 +837,7 @@ __device__ __forceinline__ int first_fit(int used) {
 
 // Round step 2: winners (JP) / every uncolored body (jacobi) take the
 // smallest free color.  JP counts the bodies still uncolored.
-__device__ void ph_round_assign(const Dev& d, bool jp, int gtid, int gsize) {
+__device__ void ph_round_assign(const Dev& d, bool jp, int* unc_out, int gtid, int gsize) {
   int unc = 0;
   for (int i = gtid; i < d.nb; i += gsize) {
     if (d.color[i] >= 0) continue;
@@ -725,7 +851,7 @@ __device__ void ph_round_assign(const Dev& d, bool jp, int gtid, int gsize) {
   }
   if (jp) {
     for (int o = 16; o > 0; o >>= 1) unc += __shfl_xor_sync(0xffffffffu, unc, o);
-    if (lane_id() == 0 && unc) atomicAdd(&d.ctr->uncolored, unc);
+    if (lane_id() == 0 && unc) atomicAdd(unc_out, unc);
   }
 }
 
@@ -741,7 +867,7 @@ __device__ void ph_resolve_edges(const Dev& d, int gtid, int gsize) {
   }
 }
 
-__device__ void ph_resolve_apply(const Dev& d, int gtid, int gsize) {
+__device__ void ph_resolve_apply(const Dev& d, int* unc_out, int gtid, int gsize) {
   int unc = 0;
   for (int i = gtid; i < d.nb; i += gsize) {
     if (d.c_lost[i]) {
@@ -751,16 +877,25 @@ __device__ void ph_resolve_apply(const Dev& d, int gtid, int gsize) {
     if (d.color[i] < 0) ++unc;
   }
   for (int o = 16; o > 0; o >>= 1) unc += __shfl_xor_sync(0xffffffffu, unc, o);
-  if (lane_id() == 0 && unc) atomicAdd(&d.ctr->uncolored, unc);
+  if (lane_id() == 0 && unc) atomicAdd(unc_out, unc);
 }
 
-// Bucketing of bodies by color, stable by body index: NCH chunks.
+// Bucketing of bodies by color.  Within a color, bodies with many incident
+// groups come first (the longest jobs start in the first wave of a pass),
+// then by body index; deterministic.  Key = 2 * color + (light ? 1 : 0).
 #define NCH 64
+#define NKEY (2 * MAX_COLORS)
+#define HEAVY_GROUPS 16
+__device__ __forceinline__ int bucket_key(const Dev& d, int i, int c) {
+  int work = (d.sg_start[i + 1] - d.sg_start[i]) + (d.dg_start[i + 1] - d.dg_start[i]);
+  return 2 * c + (work > HEAVY_GROUPS ? 0 : 1);
+}
+
 __device__ void ph_bucket_count(const Dev& d) {
-  __shared__ int h[MAX_COLORS];
+  __shared__ int h[NKEY];
   int cs = (d.nb + NCH - 1) / NCH;
   for (int b = blockIdx.x; b < NCH; b += gridDim.x) {
-    if (threadIdx.x < MAX_COLORS) h[threadIdx.x] = 0;
+    if (threadIdx.x < NKEY) h[threadIdx.x] = 0;
     __syncthreads();
     int s0 = b * cs, s1 = min(d.nb, s0 + cs);
     for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
@@ -769,67 +904,73 @@ __device__ void ph_bucket_count(const Dev& d) {
         c = 0;
         d.color[i] = 0;
       }
-      atomicAdd(&h[c], 1);
+      atomicAdd(&h[bucket_key(d, i, c)], 1);
     }
     __syncthreads();
-    if (threadIdx.x < MAX_COLORS) d.c_hist[b * MAX_COLORS + threadIdx.x] = h[threadIdx.x];
+    if (threadIdx.x < NKEY) d.c_hist[b * NKEY + threadIdx.x] = h[threadIdx.x];
     __syncthreads();
   }
 }
 
 __device__ void ph_bucket_scan(const Dev& d) {
   if (blockIdx.x != 0) return;
-  __shared__ int tot[MAX_COLORS];
-  int c = threadIdx.x;
-  if (c < MAX_COLORS) {
+  __shared__ int tot[NKEY];
+  __shared__ int kstart[NKEY + 1];
+  int k = threadIdx.x;
+  if (k < NKEY) {
     int run = 0;
     for (int b = 0; b < NCH; ++b) {
-      int v = d.c_hist[b * MAX_COLORS + c];
-      d.c_hist[b * MAX_COLORS + c] = run;
+      int v = d.c_hist[b * NKEY + k];
+      d.c_hist[b * NKEY + k] = run;
       run += v;
     }
-    tot[c] = run;
+    tot[k] = run;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     int acc = 0, mx = 0;
-    for (int k = 0; k < MAX_COLORS; ++k) {
-      d.color_starts[k] = acc;
-      acc += tot[k];
-      if (tot[k] > 0) mx = k;
+    for (int u = 0; u < NKEY; ++u) {
+      kstart[u] = acc;
+      acc += tot[u];
+      if (tot[u] > 0) mx = u >> 1;
     }
-    d.color_starts[MAX_COLORS] = acc;
+    kstart[NKEY] = acc;
+    for (int c = 0; c <= MAX_COLORS; ++c) d.color_starts[c] = kstart[2 * c < NKEY ? 2 * c : NKEY];
     d.ctr->n_colors = max(1, min(mx + 1, MAX_COLORS));
     d.ctr->color_dirty = 0;
   }
+  __syncthreads();
+  // chunk offsets become absolute positions
+  if (k < NKEY)
+    for (int b = 0; b < NCH; ++b) d.c_hist[b * NKEY + k] += kstart[k];
 }
 
 __device__ void ph_bucket_place(const Dev& d) {
-  __shared__ int run[MAX_COLORS];
-  __shared__ int wc[32][MAX_COLORS];
+  __shared__ int run[NKEY];
+  __shared__ int wc[32][NKEY];
   int cs = (d.nb + NCH - 1) / NCH;
   int w = threadIdx.x >> 5, l = lane_id();
   int nw = blockDim.x >> 5;
   for (int b = blockIdx.x; b < NCH; b += gridDim.x) {
-    if (threadIdx.x < MAX_COLORS) run[threadIdx.x] = d.color_starts[threadIdx.x] + d.c_hist[b * MAX_COLORS + threadIdx.x];
+    if (threadIdx.x < NKEY) run[threadIdx.x] = d.c_hist[b * NKEY + threadIdx.x];
     int s0 = b * cs, s1 = min(d.nb, s0 + cs);
     for (int base = s0; base < s1; base += blockDim.x) {
-      for (int k = threadIdx.x; k < 32 * MAX_COLORS; k += blockDim.x) (&wc[0][0])[k] = 0;
+      for (int k = threadIdx.x; k < 32 * NKEY; k += blockDim.x) (&wc[0][0])[k] = 0;
       __syncthreads();
       int i = base + threadIdx.x;
       bool valid = i < s1;
-      int c = valid ? d.color[i] : MAX_COLORS + l;
-      unsigned peers = __match_any_sync(0xffffffffu, c);
+      int key = valid ? bucket_key(d, i, d.color[i]) : NKEY + l;
+      unsigned peers = __match_any_sync(0xffffffffu, key);
       int rank = __popc(peers & ((1u << l) - 1u));
-      if (valid && rank == 0) wc[w][c] = __popc(peers);
+      if (valid && rank == 0) wc[w][key] = __popc(peers);
       __syncthreads();
       if (valid) {
-        int off = run[c];
-        for (int u = 0; u < w; ++u) off += wc[u][c];
+        int off = run[key];
+        for (int u = 0; u < w; ++u) off += wc[u][key];
         d.color_bodies[off + rank] = i;
       }
       __syncthreads();
-      if (threadIdx.x < MAX_COLORS) {
+      if (threadIdx.x < NKEY) {
         int t = 0;
         for (int u = 0; u < nw; ++u) t += wc[u][threadIdx.x];
         run[threadIdx.x] += t;
@@ -843,67 +984,90 @@ __device__ void ph_bucket_place(const Dev& d) {
 // The persistent substep kernel.
 // ---------------------------------------------------------------------------
 #define SOLVE_BLOCK 256
+// Two register budgets of the same kernel: 2 CTAs/SM (128 registers) or
+// 3 CTAs/SM (80 registers); the host picks one (params.blocks_per_sm).
 
-__global__ void __launch_bounds__(SOLVE_BLOCK, 1) k_solve_persistent(Dev d) {
+template <int MINB>
+__global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __grid_constant__ Dev d) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   int gsize = gridDim.x * blockDim.x;
   int bar = 0;
-#define SYNC()                               \
-  do {                                       \
-    if (!grid_barrier(d, bar++)) return;     \
-  } while (0)
   const DevParams& P = *d.prm;
+  const bool timing = P.timing != 0;
+  // SYNC(id): grid barrier; in timing mode thread 0 stamps the end of phase id.
+#define SYNC(id)                                                     \
+  do {                                                               \
+    if (!grid_barrier(d, bar++)) return;                             \
+    if (timing && gtid == 0) {                                       \
+      int m_ = d.ctr->n_marks;                                       \
+      if (m_ < 256) {                                                \
+        d.ctr->mark_t[m_] = gtimer();                                \
+        d.ctr->mark_id[m_] = (id);                                   \
+        d.ctr->n_marks = m_ + 1;                                     \
+      }                                                              \
+    }                                                                \
+  } while (0)
+  if (timing && gtid == 0) {
+    d.ctr->mark_t[0] = gtimer();
+    d.ctr->mark_id[0] = PH_START;
+    d.ctr->n_marks = 1;
+  }
   ph_gate(d, gtid, gsize);
   ph_prelude(d, gtid, gsize);  // reads x/q = the initial pose; predict runs after
-  SYNC();
+  SYNC(PH_GATE_PRELUDE);
   if (recolor_needed(d)) {
     bool jp = P.color_mode == 1;
     ph_color_reset(d, gtid, gsize);
-    SYNC();
+    SYNC(PH_COLOR_RESET);
+    // Round r counts its uncolored bodies into round_unc[r & 1]; every block
+    // reads it after the round's last barrier.  The other slot is cleared
+    // during round r's second phase, when all blocks have read it.
     int rounds = jp ? JP_ROUNDS : MAX_COLORS;
     for (int r = 0; r < rounds; ++r) {
+      int* unc_slot = &d.ctr->round_unc[r & 1];
       ph_round_edges(d, jp, gtid, gsize);
-      SYNC();
-      ph_round_assign(d, jp, gtid, gsize);
-      SYNC();
+      SYNC(PH_ROUND);
+      if (gtid == 0) d.ctr->round_unc[(r + 1) & 1] = 0;
+      ph_round_assign(d, jp, unc_slot, gtid, gsize);
+      SYNC(PH_ROUND);
       if (!jp) {
         ph_resolve_edges(d, gtid, gsize);
-        SYNC();
-        ph_resolve_apply(d, gtid, gsize);
-        SYNC();
+        SYNC(PH_ROUND);
+        ph_resolve_apply(d, unc_slot, gtid, gsize);
+        SYNC(PH_ROUND);
       }
-      int unc = *(volatile int*)&d.ctr->uncolored;
-      SYNC();  // everyone has read the count before it is reset
-      if (unc == 0) break;
-      if (gtid == 0) d.ctr->uncolored = 0;
+      if (*(volatile int*)unc_slot == 0) break;
     }
     ph_bucket_count(d);
-    SYNC();
+    SYNC(PH_BUCKET);
     ph_bucket_scan(d);
-    SYNC();
+    SYNC(PH_BUCKET);
     ph_bucket_place(d);
   } else if (gtid == 0) {
     d.ctr->recolored = 0;
   }
   ph_predict(d, gtid, gsize);
-  SYNC();
+  SYNC(PH_PREDICT);
   int iters = P.iterations;
   int total = iters + (P.post_stab ? 1 : 0);
   int nc = *(volatile int*)&d.ctr->n_colors;
+  // Pass `it` applies iteration it-1's dual update inside the color passes
+  // (owner-first), so each iteration is nc barriers; without a
+  // post-stabilization pass the last dual and the finalize run on their own.
   for (int it = 0; it < total; ++it) {
-    bool post = P.post_stab && it == iters;
+    PassMode pm = pass_mode(P, it);
     for (int c = 0; c < nc; ++c) {
-      ph_primal(d, c, post, gtid, gsize);
-      SYNC();
-    }
-    if (it < iters) {
-      ph_dual(d, it, gtid, gsize);
-      if (it == iters - 1) ph_finalize(d, gtid, gsize);
-      SYNC();
+      ph_primal(d, c, pm, gtid, gsize);
+      SYNC(PH_PRIMAL);
     }
   }
+  if (!P.post_stab && iters >= 1) {
+    ph_dual(d, iters - 1, gtid, gsize);
+    ph_finalize(d, gtid, gsize);
+    SYNC(PH_DUAL);
+  }
   ph_collect(d, gtid, gsize);
-  SYNC();
+  SYNC(PH_COLLECT);
   if (gtid == 0) {
     d.ctr->epoch += 1u;
     d.ctr->n_viol = P.record_violation ? min(iters, 64) : 0;
@@ -915,8 +1079,8 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, 1) k_solve_persistent(Dev d) {
 // Split path: one launch per phase, same phase functions.
 // ---------------------------------------------------------------------------
 #define GS int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x
-__global__ void ks_gate_prelude(Dev d) { GS; ph_gate(d, gtid, gsize); ph_prelude(d, gtid, gsize); }
-__global__ void ks_color_reset(Dev d) {
+__global__ void ks_gate_prelude(const __grid_constant__ Dev d) { GS; ph_gate(d, gtid, gsize); ph_prelude(d, gtid, gsize); }
+__global__ void ks_color_reset(const __grid_constant__ Dev d) {
   GS;
   if (!recolor_needed(d)) {
     if (gtid == 0) d.ctr->recolored = 0;
@@ -924,60 +1088,59 @@ __global__ void ks_color_reset(Dev d) {
   }
   ph_color_reset(d, gtid, gsize);
 }
-__global__ void ks_round_edges(Dev d) {
+__global__ void ks_round_edges(const __grid_constant__ Dev d) {
   GS;
   if (!d.ctr->recolored || d.ctr->uncolored < 0) return;
   ph_round_edges(d, d.prm->color_mode == 1, gtid, gsize);
 }
-__global__ void ks_round_assign(Dev d) {
+__global__ void ks_round_assign(const __grid_constant__ Dev d) {
   GS;
   if (!d.ctr->recolored || d.ctr->uncolored < 0) return;
-  ph_round_assign(d, d.prm->color_mode == 1, gtid, gsize);
+  ph_round_assign(d, d.prm->color_mode == 1, &d.ctr->uncolored, gtid, gsize);
 }
-__global__ void ks_resolve_edges(Dev d) {
+__global__ void ks_resolve_edges(const __grid_constant__ Dev d) {
   GS;
   if (!d.ctr->recolored || d.ctr->uncolored < 0 || d.prm->color_mode == 1) return;
   ph_resolve_edges(d, gtid, gsize);
 }
-__global__ void ks_resolve_apply(Dev d) {
+__global__ void ks_resolve_apply(const __grid_constant__ Dev d) {
   GS;
   if (!d.ctr->recolored || d.ctr->uncolored < 0 || d.prm->color_mode == 1) return;
-  ph_resolve_apply(d, gtid, gsize);
+  ph_resolve_apply(d, &d.ctr->uncolored, gtid, gsize);
 }
 // After a round: uncolored == 0 -> mark done (-1), else reset the count.
-__global__ void ks_round_end(Dev d) {
+__global__ void ks_round_end(const __grid_constant__ Dev d) {
   if (threadIdx.x == 0 && blockIdx.x == 0 && d.ctr->recolored && d.ctr->uncolored >= 0)
     d.ctr->uncolored = d.ctr->uncolored == 0 ? -1 : 0;
 }
-__global__ void ks_bucket_count(Dev d) {
+__global__ void ks_bucket_count(const __grid_constant__ Dev d) {
   if (!d.ctr->recolored) return;
   ph_bucket_count(d);
 }
-__global__ void ks_bucket_scan(Dev d) {
+__global__ void ks_bucket_scan(const __grid_constant__ Dev d) {
   if (!d.ctr->recolored) return;
   ph_bucket_scan(d);
 }
-__global__ void ks_bucket_place(Dev d) {
+__global__ void ks_bucket_place(const __grid_constant__ Dev d) {
   if (!d.ctr->recolored) return;
   ph_bucket_place(d);
 }
-__global__ void ks_predict(Dev d) { GS; ph_predict(d, gtid, gsize); }
-__global__ void ks_primal(Dev d, int it, int c) {
+__global__ void ks_predict(const __grid_constant__ Dev d) { GS; ph_predict(d, gtid, gsize); }
+__global__ void ks_primal(const __grid_constant__ Dev d, int it, int c) {
   GS;
   if (c >= d.ctr->n_colors) return;
-  bool post = d.prm->post_stab && it == d.prm->iterations;
-  ph_primal(d, c, post, gtid, gsize);
+  ph_primal(d, c, pass_mode(*d.prm, it), gtid, gsize);
 }
-__global__ void ks_dual(Dev d, int it) {
+__global__ void ks_tail(const __grid_constant__ Dev d) {
   GS;
   int iters = d.prm->iterations;
-  if (it < iters) {
-    ph_dual(d, it, gtid, gsize);
-    if (it == iters - 1) ph_finalize(d, gtid, gsize);
+  if (!d.prm->post_stab && iters >= 1) {
+    ph_dual(d, iters - 1, gtid, gsize);
+    ph_finalize(d, gtid, gsize);
   }
 }
-__global__ void ks_collect(Dev d) { GS; ph_collect(d, gtid, gsize); }
-__global__ void ks_end(Dev d) {
+__global__ void ks_collect(const __grid_constant__ Dev d) { GS; ph_collect(d, gtid, gsize); }
+__global__ void ks_end(const __grid_constant__ Dev d) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     d.ctr->epoch += 1u;
     d.ctr->n_viol = d.prm->record_violation ? min(d.prm->iterations, 64) : 0;
@@ -985,17 +1148,20 @@ __global__ void ks_end(Dev d) {
 }
 #undef GS
 
-int solve_occupancy(int block) {
+int solve_occupancy(int block, int variant) {
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent, block, 0);
+  if (variant >= 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<3>, block, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<2>, block, 0);
   return n;
 }
 
-cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st) {
+cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st,
+                         int variant) {
   if (persistent) {
     void* args[] = {(void*)&d};
     g_kernel_launches += 1;
-    return cudaLaunchCooperativeKernel((const void*)k_solve_persistent, dim3(grid), dim3(block), args, 0, st);
+    const void* fn = variant >= 3 ? (const void*)k_solve_persistent<3> : (const void*)k_solve_persistent<2>;
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, 0, st);
   }
   ks_gate_prelude<<<grid, block, 0, st>>>(d);
   ks_color_reset<<<grid, block, 0, st>>>(d);
@@ -1012,20 +1178,19 @@ cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, 
   ks_bucket_place<<<NCH, block, 0, st>>>(d);
   ks_predict<<<grid, block, 0, st>>>(d);
   int total = P.iterations + (P.post_stabilize ? 1 : 0);
-  for (int it = 0; it < total; ++it) {
+  for (int it = 0; it < total; ++it)
     for (int c = 0; c < MAX_COLORS; ++c) ks_primal<<<grid, block, 0, st>>>(d, it, c);
-    ks_dual<<<grid, block, 0, st>>>(d, it);
-  }
+  ks_tail<<<grid, block, 0, st>>>(d);
   ks_collect<<<grid, block, 0, st>>>(d);
   ks_end<<<1, 32, 0, st>>>(d);
-  g_kernel_launches += 2 + 5 * rounds + 3 + 1 + total * (MAX_COLORS + 1) + 2;
+  g_kernel_launches += 2 + 5 * rounds + 3 + 1 + total * MAX_COLORS + 3;
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // State reset, diagnostics, cache scrub.
 // ---------------------------------------------------------------------------
-__global__ void k_reset(Dev d) {
+__global__ void k_reset(const __grid_constant__ Dev d) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
   for (int i = gtid; i < d.nb; i += gsize) d.color[i] = -1;
   for (int s = gtid; s < d.hash_cap; s += gsize) d.h_key[s] = 0ull;
@@ -1038,12 +1203,13 @@ __global__ void k_reset(Dev d) {
     c->n_colors = MAX_COLORS;
     c->recolored = 0;
     c->bar_count = 0;
+    for (int k = 0; k < BAR_SUB; ++k) c->bar_sub[k][0] = 0;
     for (int k = 0; k < 64; ++k) c->viol_bits[k] = 0;
   }
 }
 void launch_reset(Dev& d, cudaStream_t st) { k_reset<<<148 * 4, 256, 0, st>>>(d); }
 
-__global__ void k_conflicts(Dev d, int* out) {
+__global__ void k_conflicts(const __grid_constant__ Dev d, int* out) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
   int np = d.ctr->n_pairs;
   for (int p = gtid; p < np; p += gsize) {
@@ -1064,7 +1230,7 @@ int count_conflicts(Dev& d, cudaStream_t st) {
 
 // Zero every cache slot whose tag is not the current one (keeps the live
 // entries), so tags can wrap without a stale hit.
-__global__ void k_hash_scrub(Dev d) {
+__global__ void k_hash_scrub(const __grid_constant__ Dev d) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
   unsigned tag = epoch_tag(d.ctr->epoch);
   for (int s = gtid; s < d.hash_cap; s += gsize) {
@@ -1076,11 +1242,11 @@ void launch_hash_scrub(Dev& d, cudaStream_t st) { k_hash_scrub<<<148 * 4, 256, 0
 
 // Host-provided cache contents, tagged with the current epoch so the next
 // emission finds them.
-__global__ void k_cache_clear(Dev d) {
+__global__ void k_cache_clear(const __grid_constant__ Dev d) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
   for (int s = gtid; s < d.hash_cap; s += gsize) d.h_key[s] = 0ull;
 }
-__global__ void k_cache_insert(Dev d, int n, const int* abc, const float* st) {
+__global__ void k_cache_insert(const __grid_constant__ Dev d, int n, const int* abc, const float* st) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
   unsigned tag = epoch_tag(d.ctr->epoch);
   unsigned mask = (unsigned)d.hash_cap - 1u;

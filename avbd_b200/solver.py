@@ -213,6 +213,7 @@ class Solver6DOF:
         self.use_graph = bool(use_graph)
         self.record_violation = False
         self.blocks_per_sm = 0
+        self.timing = False  # stamp the solve kernel's phases (phase_profile())
         self._debug_skip_arrive = False
         self._mlp = mlp_warm_start
 
@@ -511,6 +512,7 @@ class Solver6DOF:
         self._ctx = ctx
         st = self._stream()
         _lib.check(L.avbd_reset_state(self._ctx, st), "reset")
+        self._pushed = None  # a new context starts without parameters
         self._push_params()
         self._gpu_pool_n_static = len(self._rows)
         self._gpu_pool_n_dyn_capacity = dims.dyn_row_cap
@@ -546,6 +548,7 @@ class Solver6DOF:
         p.mlp_warm_start = int(self._mlp is not None and getattr(self._mlp, "enabled", True))
         p.debug_skip_arrive = int(self._debug_skip_arrive)
         p.blocks_per_sm = int(self.blocks_per_sm)
+        p.timing = int(self.timing)
         return p
 
     def _push_params(self):
@@ -671,6 +674,20 @@ class Solver6DOF:
             return 0
         return int(_lib.load().avbd_count_color_conflicts(self._ctx, self._stream()))
 
+    def phase_profile(self) -> dict:
+        """Device time (ms) per phase of the last substep's persistent solve
+        kernel and the number of grid barriers of each (needs timing=True)."""
+        cap = 256
+        t = (C.c_longlong * cap)()
+        ph = (C.c_int * cap)()
+        n = _lib.check(_lib.load().avbd_read_phase_marks(self._ctx, t, ph, cap, self._stream()), "phase marks")
+        out = {}
+        for k in range(1, n):
+            name = _lib.PHASES[ph[k]] if 0 <= ph[k] < len(_lib.PHASES) else str(ph[k])
+            ms, cnt = out.get(name, (0.0, 0))
+            out[name] = (ms + (t[k] - t[k - 1]) * 1e-6, cnt + 1)
+        return out
+
     def clear_errors(self) -> None:
         """Clear the sticky device error bits (after handling a reported error)."""
         if self._ctx is not None:
@@ -794,22 +811,25 @@ class Solver6DOF:
         return out
 
     # ---- in-place setters (solver_6dof.py:878-900) -------------------------------
+    # They write into the existing device buffers (never rebind them), so
+    # captured CUDA graphs keep operating on the live state.
     @_on_stream
-    def _set_row(self, t: torch.Tensor, idx: int, vals) -> None:
+    def _set_row(self, name: str, idx: int, vals) -> None:
         self._flush()
+        t = getattr(self, name)
         t[idx, : len(vals)] = torch.tensor([float(v) for v in vals], dtype=torch.float32, device=self.device)
 
     def set_position(self, body, p) -> None:
-        self._set_row(self.x4, body.index, p)
+        self._set_row("x4", body.index, p)
 
     def set_orientation(self, body, q_xyzw) -> None:
-        self._set_row(self.q, body.index, q_xyzw)
+        self._set_row("q", body.index, q_xyzw)
 
     def set_velocity(self, body, v) -> None:
-        self._set_row(self.v4, body.index, v)
+        self._set_row("v4", body.index, v)
 
     def set_angular_velocity(self, body, w) -> None:
-        self._set_row(self.w4, body.index, w)
+        self._set_row("w4", body.index, w)
 
     @_on_stream
     def upload_body_state(self, x4, q, v4=None, w4=None) -> None:

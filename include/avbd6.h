@@ -77,6 +77,7 @@ typedef struct AvbdParams {
   int mlp_warm_start;  /* 1 = learned warm start for new contacts */
   int debug_skip_arrive; /* test hook: block 0 skips one barrier arrival */
   int blocks_per_sm;   /* persistent grid: CTAs per SM (0 = occupancy max) */
+  int timing;          /* stamp the persistent kernel's phase boundaries */
 } AvbdParams;
 
 typedef struct AvbdStats {
@@ -140,6 +141,10 @@ int avbd_clear_errors(AvbdCtx* ctx, void* stream);
 /* Device time of the last substep's collision and solve parts, in ms
  * (replaces broadphase_ms, solver_6dof.py:1786-1787, 1916).  Synchronises. */
 int avbd_step_ms(AvbdCtx* ctx, float* collide_ms, float* solve_ms);
+
+/* Phase timestamps of the last substep's solve (params.timing = 1): up to
+ * `cap` (globaltimer ns, phase id) pairs; returns the count.  Synchronises. */
+int avbd_read_phase_marks(AvbdCtx* ctx, long long* t_ns, int* phase, int cap, void* stream);
 
 /* Last error text of this thread. */
 const char* avbd_last_error(void);
