@@ -73,6 +73,8 @@ def load():
     L.avbd_clear_errors.argtypes = [vp, vp]
     L.avbd_step_ms.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.avbd_read_phase_marks.argtypes = [vp, vp, vp, i, vp]
+    L.avbd_exclusive_scan_noalloc.argtypes = [vp, vp, i, vp]
+    L.avbd_exclusive_scan_noalloc.restype = i
     for name in ("avbd_layout", "avbd_create", "avbd_destroy", "avbd_set_params", "avbd_reset_state",
                  "avbd_mark_color_dirty", "avbd_substep", "avbd_step", "avbd_read_stats",
                  "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors", "avbd_step_ms",
@@ -93,7 +95,7 @@ def check(code: int, what: str) -> int:
 EXPORTED = ["avbd_num_arrays", "avbd_array_name", "avbd_layout", "avbd_create", "avbd_destroy",
             "avbd_set_params", "avbd_reset_state", "avbd_mark_color_dirty", "avbd_substep", "avbd_step",
             "avbd_read_stats", "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors",
-            "avbd_step_ms", "avbd_read_phase_marks", "avbd_last_error"]
+            "avbd_step_ms", "avbd_read_phase_marks", "avbd_exclusive_scan_noalloc", "avbd_last_error"]
 
 PHASES = ["start", "gate+prelude", "color reset", "color rounds", "bucket", "predict", "primal", "dual",
           "collect"]

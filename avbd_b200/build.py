@@ -23,6 +23,7 @@ UNITS = {
     "solve.cu": [],
     "api.cu": [],
     "mlp.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -86,6 +86,11 @@ bool compute_layout(const AvbdDims* dm, size_t* off, size_t* total) {
 
 }  // namespace
 
+namespace avbd {
+// Error text for entry points defined in other translation units.
+void set_error_text(const char* what, cudaError_t e) { fail(0, what, e); }
+}  // namespace avbd
+
 struct AvbdCtx {
   AvbdDims dims;
   AvbdParams P;

@@ -146,6 +146,17 @@ int avbd_step_ms(AvbdCtx* ctx, float* collide_ms, float* solve_ms);
  * `cap` (globaltimer ns, phase id) pairs; returns the count.  Synchronises. */
 int avbd_read_phase_marks(AvbdCtx* ctx, long long* t_ns, int* phase, int cap, void* stream);
 
+/* Exclusive prefix sum of n int32 (out[0..n], out[n] = total) that allocates
+ * no device memory.  No counterpart in the reference: it serves callers that
+ * cannot call cudaMalloc (a host that owns the device-memory budget, a
+ * real-time loop).  Its scratch is a fixed 16 KiB device array of this
+ * library, so n is limited to 8,388,607 (larger n returns AVBD_E_INVALID).
+ * The first call on a device looks the array up (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls on a device share the
+ * array: calls that overlap on the GPU race, so serialise them.  `in` and
+ * `out` are device pointers; asynchronous on `stream`. */
+int avbd_exclusive_scan_noalloc(const int* in, int* out, int n, void* stream);
+
 /* Last error text of this thread. */
 const char* avbd_last_error(void);
 
