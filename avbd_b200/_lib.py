@@ -20,7 +20,7 @@ AVBD_ERR_BVH = 64
 class AvbdDims(C.Structure):
     _fields_ = [("n_bodies", C.c_int), ("n_static_groups", C.c_int), ("n_static_rows", C.c_int),
                 ("pair_cap", C.c_int), ("dyn_row_cap", C.c_int), ("dyn_group_cap", C.c_int),
-                ("hash_cap", C.c_int), ("mlp_floats", C.c_int)]
+                ("hash_cap", C.c_int), ("mlp_floats", C.c_int), ("new_cap", C.c_int)]
 
 
 class AvbdParams(C.Structure):
@@ -31,7 +31,7 @@ class AvbdParams(C.Structure):
                 ("recolor_every_substep", C.c_int), ("self_collide", C.c_int), ("self_friction", C.c_float),
                 ("group_size", C.c_int), ("use_graph", C.c_int), ("persistent", C.c_int),
                 ("record_violation", C.c_int), ("mlp_warm_start", C.c_int), ("debug_skip_arrive", C.c_int),
-                ("blocks_per_sm", C.c_int), ("timing", C.c_int)]
+                ("blocks_per_sm", C.c_int), ("timing", C.c_int), ("log_new_contacts", C.c_int)]
 
 
 class AvbdStats(C.Structure):
@@ -40,7 +40,15 @@ class AvbdStats(C.Structure):
                 ("n_colors", C.c_int), ("recolored", C.c_int), ("conflicts", C.c_int), ("err", C.c_int),
                 ("err_where", C.c_int), ("n_cache_hits", C.c_int), ("n_new_contacts", C.c_int),
                 ("max_dg", C.c_int), ("n_viol", C.c_int), ("epoch", C.c_uint), ("graph_state", C.c_int),
-                ("capture_err", C.c_int), ("kernels_launched", C.c_longlong), ("viol", C.c_float * 64)]
+                ("capture_err", C.c_int), ("kernels_launched", C.c_longlong), ("viol", C.c_float * 64),
+                ("n_new_logged", C.c_int), ("n_mlp_applied", C.c_int), ("n_mlp_fallback", C.c_int),
+                ("viol_contact", C.c_float * 64)]
+
+# Learned warm-start network sizes (avbd6.h AVBD_MLP_*).
+MLP_IN = 20
+MLP_OUT = 4
+MLP_PARAMS = 5764
+MLP_FLOATS = 3544
 
 
 _lib = None
@@ -75,10 +83,16 @@ def load():
     L.avbd_read_phase_marks.argtypes = [vp, vp, vp, i, vp]
     L.avbd_exclusive_scan_noalloc.argtypes = [vp, vp, i, vp]
     L.avbd_exclusive_scan_noalloc.restype = i
+    L.avbd_mlp_pack.argtypes = [vp, vp, vp, vp]
+    L.avbd_mlp_infer.argtypes = [vp, vp, i, vp, vp]
+    L.avbd_mlp_scratch_bytes.argtypes = [i]
+    L.avbd_mlp_scratch_bytes.restype = sz
+    L.avbd_mlp_loss_grad.argtypes = [vp, vp, vp, i, vp, vp, vp, sz, vp]
+    L.avbd_mlp_adam.argtypes = [vp, vp, vp, vp, i, C.c_float, C.c_float, C.c_float, C.c_float, vp]
     for name in ("avbd_layout", "avbd_create", "avbd_destroy", "avbd_set_params", "avbd_reset_state",
                  "avbd_mark_color_dirty", "avbd_substep", "avbd_step", "avbd_read_stats",
                  "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors", "avbd_step_ms",
-                 "avbd_read_phase_marks"):
+                 "avbd_read_phase_marks", "avbd_mlp_pack", "avbd_mlp_infer", "avbd_mlp_loss_grad", "avbd_mlp_adam"):
         getattr(L, name).restype = i
     _lib = L
     return L
@@ -95,7 +109,8 @@ def check(code: int, what: str) -> int:
 EXPORTED = ["avbd_num_arrays", "avbd_array_name", "avbd_layout", "avbd_create", "avbd_destroy",
             "avbd_set_params", "avbd_reset_state", "avbd_mark_color_dirty", "avbd_substep", "avbd_step",
             "avbd_read_stats", "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors",
-            "avbd_step_ms", "avbd_read_phase_marks", "avbd_exclusive_scan_noalloc", "avbd_last_error"]
+            "avbd_step_ms", "avbd_read_phase_marks", "avbd_exclusive_scan_noalloc", "avbd_mlp_pack",
+            "avbd_mlp_infer", "avbd_mlp_scratch_bytes", "avbd_mlp_loss_grad", "avbd_mlp_adam", "avbd_last_error"]
 
 PHASES = ["start", "gate+prelude", "color reset", "color rounds", "bucket", "predict", "primal", "dual",
           "collect"]

@@ -42,7 +42,8 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(PAIR_GCNT, 4, P) X(PAIR_GSTART, 4, P + 1) X(PAIR_RSTART, 4, P + 1) X(PAIR_KEPT, 4, P + 1) X(H_KEY, 8, H)   \
   X(H_S0, 16, H) X(H_S1, 16, H) X(SCAN_PART, 4, SP) X(SORT_HIST, 4, SH) X(C_USED, 4, N) X(C_LOST, 4, N)        \
   X(C_HIST, 4, 64 * 64) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
-  X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS)
+  X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
+  X(MLP_FEAT, 4, NC * MLP_IN)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,
@@ -58,7 +59,8 @@ const char* kNames[] = {
 
 bool compute_layout(const AvbdDims* dm, size_t* off, size_t* total) {
   if (!dm || dm->n_bodies < 0 || dm->n_static_groups < 0 || dm->pair_cap < 0 || dm->dyn_group_cap < 0 ||
-      dm->dyn_row_cap < 0 || dm->hash_cap < 1 || (dm->hash_cap & (dm->hash_cap - 1)) != 0 || dm->mlp_floats < 0)
+      dm->dyn_row_cap < 0 || dm->hash_cap < 1 || (dm->hash_cap & (dm->hash_cap - 1)) != 0 ||
+      (dm->mlp_floats != 0 && dm->mlp_floats != AVBD_MLP_FLOATS) || dm->new_cap < 0)
     return false;
   long long N = dm->n_bodies > 0 ? dm->n_bodies : 1;
   long long DG = dm->dyn_group_cap;
@@ -67,6 +69,7 @@ bool compute_layout(const AvbdDims* dm, size_t* off, size_t* total) {
   long long P = dm->pair_cap > 0 ? dm->pair_cap : 1;
   long long H = dm->hash_cap;
   long long M = dm->mlp_floats;
+  long long NC = dm->new_cap;
   long long nblk = (N + 2047) / 2048;
   long long SH = 256 * nblk + 1;
   long long big = P > SH ? P : SH;
@@ -194,6 +197,9 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.scan_part = PTR(int*, SCAN_PART); d.sort_hist = PTR(int*, SORT_HIST);
   d.c_used = PTR(int*, C_USED); d.c_lost = PTR(int*, C_LOST); d.c_hist = PTR(int*, C_HIST);
   d.mlp_w = dims->mlp_floats > 0 ? PTR(const float*, MLP_W) : nullptr;
+  d.new_cap = dims->new_cap;
+  d.new_list = PTR(int*, NEW_LIST);
+  d.mlp_feat = PTR(float*, MLP_FEAT);
   d.ctr = PTR(DevCounters*, COUNTERS);
 #undef PTR
   int occ = solve_occupancy(256, 2);
@@ -247,7 +253,8 @@ static void fill_devparams(AvbdCtx* c, float dt_sub) {
   q.group_size = (g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32) ? g : 16;
   q.record_violation = P.record_violation;
   q.debug_skip_arrive = P.debug_skip_arrive;
-  q.mlp_on = P.mlp_warm_start && c->dims.mlp_floats > 0;
+  q.mlp_on = P.mlp_warm_start && c->dims.mlp_floats > 0 && c->dims.new_cap > 0;
+  q.log_new = P.log_new_contacts && c->dims.new_cap > 0;
   q.barrier_timeout_ns = P.debug_skip_arrive ? 200000000ull : 2000000000ull;
   q.timing = P.timing;
 }
@@ -421,6 +428,10 @@ int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {
   out->graph_state = (c->graph_ok[0] ? 1 : 0) | (c->graph_ok[1] ? 2 : 0);
   out->capture_err = c->capture_err[0] * 1000 + c->capture_err[1];
   out->kernels_launched = c->kernels_launched;
+  out->n_new_logged = h.n_new_logged;
+  out->n_mlp_applied = h.n_mlp_applied;
+  out->n_mlp_fallback = h.n_mlp_fallback;
+  for (int k = 0; k < 64; ++k) out->viol_contact[k] = h.vc_cnt[k] > 0 ? h.vc_sum[k] / (float)h.vc_cnt[k] : 0.0f;
   for (int k = 0; k < 64; ++k) {
     unsigned b = h.viol_bits[k];
     float f;
@@ -429,7 +440,6 @@ int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {
   }
   if (h.err & AVBD_ERR_BARRIER_TIMEOUT) return fail(AVBD_E_TIMEOUT, "device barrier timed out");
   return settle_errors(AVBD_OK, "read_stats");
-  return AVBD_OK;
 }
 
 int avbd_cache_load(AvbdCtx* c, int n, const int* abc, const float* state, void* stream) {

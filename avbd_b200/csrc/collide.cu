@@ -41,11 +41,18 @@ __global__ void k_begin_substep(const __grid_constant__ Dev d) {
     c->conflicts = 0;
     c->n_cache_hits = 0;
     c->n_new_contacts = 0;
+    c->n_new_logged = 0;
+    c->n_mlp_applied = 0;
+    c->n_mlp_fallback = 0;
     c->max_dg = 0;
     c->n_viol = 0;
     c->bar_count = 0;
     for (int k = 0; k < BAR_SUB; ++k) c->bar_sub[k][0] = 0;
-    for (int k = 0; k < 64; ++k) c->viol_bits[k] = 0;
+    for (int k = 0; k < 64; ++k) {
+      c->viol_bits[k] = 0;
+      c->vc_sum[k] = 0.0f;
+      c->vc_cnt[k] = 0;
+    }
     int* b = (int*)d.bounds;
     b[0] = b[1] = b[2] = 0x7fffffff;
     b[3] = b[4] = b[5] = (int)0x80000000;
@@ -467,6 +474,7 @@ struct Manifold {
   float depth;
   V3 nn;  // contact normal (inc -> ref)
   V3 off_ref[4], off_inc[4];
+  float pen[4];  // penetration depth of each contact (>0 when penetrating)
 };
 
 __device__ void sat_manifold(V3 cA, M3 RA, V3 eA, V3 cB, M3 RB, V3 eB, Manifold& o) {
@@ -570,6 +578,7 @@ __device__ void sat_manifold(V3 cA, M3 RA, V3 eA, V3 cB, M3 RB, V3 eB, Manifold&
     o.nn = ba;
     o.off_ref[0] = mtv(RA, pA - cA);
     o.off_inc[0] = mtv(RB, pB - cB);
+    o.pen[0] = -gap;
     return;
   }
   // face-face: Sutherland-Hodgman clip of the incident face by the
@@ -674,6 +683,7 @@ __device__ void sat_manifold(V3 cA, M3 RA, V3 eA, V3 cB, M3 RB, V3 eB, Manifold&
     V3 pr = pi - rfn * ds;
     o.off_ref[c] = mtv(Rr, pr - ref_c);
     o.off_inc[c] = mtv(Ri, pi - inc_c);
+    o.pen[c] = bdp[c];
   }
 }
 
@@ -690,7 +700,7 @@ __global__ void k_narrow(const __grid_constant__ Dev d) {
     d.pair_info[p] = o.overlap | ((o.sat_idx & 31) << 1) | (o.count << 6) | (o.ref_is_a << 9);
     d.pair_nrm[p] = make_float4(o.nn.x, o.nn.y, o.nn.z, o.depth);
     for (int c = 0; c < o.count; ++c) {
-      d.pair_off[8 * p + c] = make_float4(o.off_ref[c].x, o.off_ref[c].y, o.off_ref[c].z, 0.0f);
+      d.pair_off[8 * p + c] = make_float4(o.off_ref[c].x, o.off_ref[c].y, o.off_ref[c].z, o.pen[c]);
       d.pair_off[8 * p + 4 + c] = make_float4(o.off_inc[c].x, o.off_inc[c].y, o.off_inc[c].z, 0.0f);
     }
     // friction of the contact (kernels_6dof.py:2775-2780): sqrt(mu_ref mu_inc)
@@ -716,6 +726,51 @@ __device__ __forceinline__ int cache_find(const Dev& d, unsigned long long k, un
     if ((unsigned)(v >> 50) != tag) return -1;
   }
   return -1;
+}
+
+// The 20 inputs of the learned warm start for one new contact (ref body a,
+// incident body b): normal in a's frame (3), penetration depth (1), relative
+// contact-point velocity in the (t, b, n) contact frame (3), inverse masses
+// (2), n^T I^-1 n of both bodies (2), mu_s, mu_d (2), one-hot SAT axis class
+// of the pair, A being its lower body index (face of A x/y/z, face of B
+// x/y/z, edge-edge) (7).
+__device__ void contact_features(const Dev& d, int a, int b, float4 nn, float4 offa, float4 offb, int sat, float mu,
+                                 float mus, float* out) {
+  V3 n = xyz(nn);
+  float4 xa = d.x[a], xb = d.x[b];
+  M3 Ra = qmat(d.q[a]), Rb = qmat(d.q[b]);
+  V3 na = mtv(Ra, n), nb = mtv(Rb, n);
+  V3 ra = V3{Ra.m[0][0] * offa.x + Ra.m[0][1] * offa.y + Ra.m[0][2] * offa.z,
+             Ra.m[1][0] * offa.x + Ra.m[1][1] * offa.y + Ra.m[1][2] * offa.z,
+             Ra.m[2][0] * offa.x + Ra.m[2][1] * offa.y + Ra.m[2][2] * offa.z};
+  V3 rb = V3{Rb.m[0][0] * offb.x + Rb.m[0][1] * offb.y + Rb.m[0][2] * offb.z,
+             Rb.m[1][0] * offb.x + Rb.m[1][1] * offb.y + Rb.m[1][2] * offb.z,
+             Rb.m[2][0] * offb.x + Rb.m[2][1] * offb.y + Rb.m[2][2] * offb.z};
+  V3 va = xyz(d.v[a]) + cross(xyz(d.w[a]), ra);
+  V3 vb = xyz(d.v[b]) + cross(xyz(d.w[b]), rb);
+  V3 vr = va - vb;
+  V3 t = orthonormal_basis(n);
+  V3 bt = cross(n, t);
+  float4 ia = d.iloc[a], ib = d.iloc[b];
+  float nia = (ia.x > 0.0f ? na.x * na.x / ia.x : 0.0f) + (ia.y > 0.0f ? na.y * na.y / ia.y : 0.0f) +
+              (ia.z > 0.0f ? na.z * na.z / ia.z : 0.0f);
+  float nib = (ib.x > 0.0f ? nb.x * nb.x / ib.x : 0.0f) + (ib.y > 0.0f ? nb.y * nb.y / ib.y : 0.0f) +
+              (ib.z > 0.0f ? nb.z * nb.z / ib.z : 0.0f);
+  out[0] = na.x;
+  out[1] = na.y;
+  out[2] = na.z;
+  out[3] = offa.w;
+  out[4] = dot(vr, t);
+  out[5] = dot(vr, bt);
+  out[6] = dot(vr, n);
+  out[7] = xa.w > 0.0f ? 1.0f / xa.w : 0.0f;
+  out[8] = xb.w > 0.0f ? 1.0f / xb.w : 0.0f;
+  out[9] = nia;
+  out[10] = nib;
+  out[11] = mus;
+  out[12] = mu;
+  int cls = sat < 6 ? sat : 6;
+  for (int k = 0; k < 7; ++k) out[13 + k] = k == cls ? 1.0f : 0.0f;
 }
 
 // Emission (kernels_6dof.py:2695-2912): one contact group per contact, rows
@@ -758,6 +813,15 @@ __global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_g
           s0 = d.h_s0[slot];
           s1 = d.h_s1[slot];
           ++hits;
+        } else if (d.prm->mlp_on || d.prm->log_new) {
+          // A new contact: queue it (with its features) for the learned
+          // warm start or for the training log.
+          int k = atomicAdd(&d.ctr->n_new_logged, 1);
+          if (k < d.new_cap) {
+            d.new_list[k] = g;
+            contact_features(d, ref, inc, nn, d.pair_off[8 * p + c], d.pair_off[8 * p + 4 + c], (info >> 1) & 31, mu,
+                             mus, d.mlp_feat + (size_t)MLP_IN * k);
+          }
         }
         d.g_lam[g] = make_float4(s0.x, s0.y, s0.z, 0.0f);
         d.g_pen[g] = make_float4(s0.w, s1.x, s1.y, 0.0f);
@@ -858,6 +922,7 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
   k_dg_fill<<<grid, 256, 0, st>>>(d);
   k_dg_sort<<<grid, 128, 0, st>>>(d);
   g_kernel_launches += 13;  // the direct launches above (scans and sort count themselves)
+  if (dims.mlp_floats > 0 && dims.new_cap > 0) launch_mlp_warm(d, st);
 }
 
 }  // namespace avbd

@@ -42,6 +42,23 @@ enum : int { FL_ACT0 = 1, FL_ACT1 = 2, FL_ACT2 = 4, FL_WAS = 8, FL_WAST = 16, FL
 #define COLL_MARGIN 0.005f
 #define BP_SLOTS 32
 
+// Learned warm start: layer widths and the packed inference block (floats;
+// layout documented with AVBD_MLP_FLOATS in avbd6.h).
+#define MLP_IN AVBD_MLP_IN
+#define MLP_H 64
+#define MLP_OUT AVBD_MLP_OUT
+#define MLPO_FMEAN 0
+#define MLPO_FISTD 32
+#define MLPO_OMEAN 64
+#define MLPO_OSTD 72
+#define MLPO_B1 80
+#define MLPO_B2 144
+#define MLPO_B3 208
+#define MLPO_W1 216   // bf16 [64][32] as 1024 bf16 pairs
+#define MLPO_W2 1240  // bf16 [64][64] as 2048 pairs
+#define MLPO_W3 3288  // bf16 [8][64] as 256 pairs
+static_assert(MLPO_W3 + 256 == AVBD_MLP_FLOATS, "packed MLP block size");
+
 // Error bits of the device status word.
 enum : int {
   ERR_BARRIER_TIMEOUT = 1,
@@ -76,7 +93,10 @@ struct DevCounters {
   unsigned viol_bits[64];  // per-iteration max violation (float bits, >= 0)
   int n_viol;
   int n_marks;           // phase timestamps recorded (timing mode)
-  int pad[14];
+  int n_new_logged;      // new contacts queued for the learned warm start / log
+  int n_mlp_applied;     // new contacts that took the learned warm start
+  int n_mlp_fallback;    // new contacts that fell back to the zero start
+  int pad[11];
   unsigned long long mark_t[256];  // globaltimer after each grid barrier
   int mark_id[256];                // phase id of that barrier (PH_*)
   // grid barrier state (each counter on its own 128-byte line): blocks
@@ -89,6 +109,8 @@ struct DevCounters {
   unsigned bar_sub[16][32];
   int round_unc[2];  // uncolored counts of alternate coloring rounds
   int pad4[30];
+  float vc_sum[64];  // per-iteration violation sum over box-box contact groups
+  int vc_cnt[64];    // and their count (record_violation)
 };
 #define BAR_SUB 16
 
@@ -110,8 +132,9 @@ struct DevParams {
   int debug_skip_arrive;
   int mlp_on;
   unsigned long long barrier_timeout_ns;
-  int timing;  // record phase timestamps in the counters
-  int pad[7];
+  int timing;   // record phase timestamps in the counters
+  int log_new;  // queue every new contact's features (training-data log)
+  int pad[6];
 };
 
 // Phase ids of the persistent kernel's timestamps.
@@ -163,6 +186,9 @@ struct Dev {
   int *c_used, *c_lost, *c_hist;
   // learned warm start (optional): packed weights, null when disabled
   const float* mlp_w;
+  int new_cap;      // capacity of the new-contact queue
+  int* new_list;    // group id of each queued new contact
+  float* mlp_feat;  // MLP_IN raw features of each queued new contact
   // counters
   DevCounters* ctr;
 };

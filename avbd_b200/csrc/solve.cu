@@ -180,7 +180,8 @@ __device__ __forceinline__ void acc_axis(Acc& s, V3 rs, float f, float kl) {
 // Dual update of one group's rows in row order (kernels_6dof.py:1451-1548):
 // a friction row sees its normal row's new lambda and was_static flag.
 // Craw are the rows' constraint values at the current pose; ac the stored
-// alpha*C0.  Returns the largest violation of the non-friction rows.
+// alpha*C0.  Returns the largest violation of the non-friction rows, measured
+// on the value the update drives (C - alpha*C0 for hard rows).
 __device__ __forceinline__ float dual_rows(int kind, int nr, bool hard, float4 mat, const float* Craw, const float* ac,
                                            float beta, float* lm, float* pn, int& fl) {
   bool tang = kind != KIND_PIN;
@@ -205,7 +206,7 @@ __device__ __forceinline__ float dual_rows(int kind, int nr, bool hard, float4 m
     } else {
       lo = -FINF;
       hi = kind == KIND_PIN ? FINF : 0.0f;
-      vmax = fmaxf(vmax, kind == KIND_PIN ? fabsf(Craw[k]) : fmaxf(0.0f, -Craw[k]));
+      vmax = fmaxf(vmax, kind == KIND_PIN ? fabsf(C) : fmaxf(0.0f, -C));
     }
     float nl = fminf(fmaxf(pn[k] * C + le, lo), hi);
     lm[k] = nl;
@@ -229,9 +230,10 @@ __device__ __forceinline__ float dual_rows(int kind, int nr, bool hard, float4 m
 // color), the previous iteration's dual update of g is applied first: both
 // bodies still hold their poses from the end of that iteration, because the
 // owner's color runs before the other body's.  Returns the violation of the
-// updated rows (0 when no dual ran).
+// updated rows (0 when no dual ran); a box-box group's violation is also
+// added to csum / ccnt (the contact-row statistics of record_violation).
 __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3 xi, float4 qi, bool post, bool dual,
-                                                  Acc& s) {
+                                                  Acc& s, float& csum, int& ccnt) {
   int meta = d.g_meta[g];
   int fl = d.g_flags[g];
   int kind = meta_kind(meta);
@@ -289,6 +291,10 @@ __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3
     d.g_lam[g] = make_float4(lm[0], lm[1], lm[2], 0.0f);
     d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
     d.g_flags[g] = fl;
+    if (kind == KIND_BOX && (fl & FL_ACT0)) {
+      csum += viol;
+      ++ccnt;
+    }
   }
   if (post) {  // post-stabilization pass: alpha = 0 for non-friction rows (kernels_6dof.py:1733-1811)
     ac[0] = 0.0f;
@@ -454,6 +460,24 @@ struct PassMode {
   int viol_slot;  // iteration whose violation is recorded (-1: none)
 };
 
+// Folds a warp's violation statistics of iteration `slot` into the
+// counters: the max over all rows, and the sum / count over box-box contact
+// groups (their mean is the contact-row statistic).
+__device__ __forceinline__ void record_violation(const Dev& d, int slot, float vmax, float csum, int ccnt) {
+  for (int o = 16; o > 0; o >>= 1) {
+    vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    csum += __shfl_xor_sync(0xffffffffu, csum, o);
+    ccnt += __shfl_xor_sync(0xffffffffu, ccnt, o);
+  }
+  if (lane_id() == 0) {
+    if (vmax > 0.0f) atomicMax(&d.ctr->viol_bits[slot], __float_as_uint(vmax));
+    if (ccnt > 0) {
+      atomicAdd(&d.ctr->vc_sum[slot], csum);
+      atomicAdd(&d.ctr->vc_cnt[slot], ccnt);
+    }
+  }
+}
+
 // Primal sweep of one color: G lanes per body, butterfly reduction of the
 // 27 accumulators, lane 0 solves (kernels_6dof.py:1149-1414, in place).
 template <int G>
@@ -461,7 +485,8 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
   int cs0 = d.color_starts[c];
   int nbody = d.color_starts[c + 1] - cs0;
   int total = nbody * G;
-  float vmax = 0.0f;
+  float vmax = 0.0f, csum = 0.0f;
+  int ccnt = 0;
   for (int base = 0; base < total; base += gsize) {
     int t = base + gtid;
     int slot = t / G, lane = t & (G - 1);
@@ -486,7 +511,7 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
       }
       for (int k = lane; k < ns + nd; k += G) {
         int g = k < ns ? s0 + k : d.dg_idx[e0 + (k - ns)];
-        vmax = fmaxf(vmax, accumulate_group(d, g, i, xi, qi, pm.post, pm.dual, s));
+        vmax = fmaxf(vmax, accumulate_group(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt));
       }
     }
     if (G > 1) {
@@ -508,10 +533,7 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
     }
     if (act && lane == 0) solve_body(d, i, xi4, qi, s, dt);
   }
-  if (pm.viol_slot >= 0) {
-    for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-    if (lane_id() == 0 && vmax > 0.0f) atomicMax(&d.ctr->viol_bits[pm.viol_slot], __float_as_uint(vmax));
-  }
+  if (pm.viol_slot >= 0) record_violation(d, pm.viol_slot, vmax, csum, ccnt);
 }
 
 __device__ void ph_primal(const Dev& d, int c, PassMode pm, int gtid, int gsize) {
@@ -639,7 +661,8 @@ __device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
 __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
   const DevParams& P = *d.prm;
   int ng = n_groups_live(d);
-  float vmax = 0.0f;
+  float vmax = 0.0f, csum = 0.0f;
+  int ccnt = 0;
   for (int g = gtid; g < ng; g += gsize) {
     int meta = d.g_meta[g];
     int fl = d.g_flags[g];
@@ -649,15 +672,17 @@ __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
     float4 lam = d.g_lam[g], pen = d.g_pen[g], ac0 = d.g_ac0[g], mat = d.g_mat[g];
     GroupC cv = group_values(d, g, meta, d.x, d.q);
     float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z}, ac[3] = {ac0.x, ac0.y, ac0.z};
-    vmax = fmaxf(vmax, dual_rows(kind, three ? 3 : 1, hard, mat, cv.c, ac, P.beta, lm, pn, fl));
+    float v = dual_rows(kind, three ? 3 : 1, hard, mat, cv.c, ac, P.beta, lm, pn, fl);
+    vmax = fmaxf(vmax, v);
+    if (kind == KIND_BOX && (fl & FL_ACT0)) {
+      csum += v;
+      ++ccnt;
+    }
     d.g_lam[g] = make_float4(lm[0], lm[1], lm[2], 0.0f);
     d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
     d.g_flags[g] = fl;
   }
-  if (P.record_violation && it < 64) {
-    for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-    if (lane_id() == 0 && vmax > 0.0f) atomicMax(&d.ctr->viol_bits[it], __float_as_uint(vmax));
-  }
+  if (P.record_violation && it < 64) record_violation(d, it, vmax, csum, ccnt);
 }
 
 // Inertial target + warm start (kernels_6dof.py:122-187), plus the owner of
@@ -1204,7 +1229,11 @@ __global__ void k_reset(const __grid_constant__ Dev d) {
     c->recolored = 0;
     c->bar_count = 0;
     for (int k = 0; k < BAR_SUB; ++k) c->bar_sub[k][0] = 0;
-    for (int k = 0; k < 64; ++k) c->viol_bits[k] = 0;
+    for (int k = 0; k < 64; ++k) {
+      c->viol_bits[k] = 0;
+      c->vc_sum[k] = 0.0f;
+      c->vc_cnt[k] = 0;
+    }
   }
 }
 void launch_reset(Dev& d, cudaStream_t st) { k_reset<<<148 * 4, 256, 0, st>>>(d); }

@@ -216,6 +216,7 @@ class Solver6DOF:
         self.timing = False  # stamp the solve kernel's phases (phase_profile())
         self._debug_skip_arrive = False
         self._mlp = mlp_warm_start
+        self._log_new = False
 
         self._x, self._q, self._v, self._omega = [], [], [], []
         self._mass, self._half_extents, self._friction = [], [], []
@@ -379,6 +380,9 @@ class Solver6DOF:
         d.dyn_group_cap = dr
         d.hash_cap = hc
         d.mlp_floats = 0 if self._mlp is None else int(self._mlp.n_floats)
+        # new-contact queue: allocated only when a warm-start model or the
+        # training log can use it
+        d.new_cap = max(1024, 8 * n) if self._self_collide and (self._mlp is not None or self._log_new) else 0
         return d
 
     def _views(self):
@@ -549,6 +553,7 @@ class Solver6DOF:
         p.debug_skip_arrive = int(self._debug_skip_arrive)
         p.blocks_per_sm = int(self.blocks_per_sm)
         p.timing = int(self.timing)
+        p.log_new_contacts = int(self._log_new)
         return p
 
     def _push_params(self):
@@ -694,13 +699,78 @@ class Solver6DOF:
             _lib.check(_lib.load().avbd_clear_errors(self._ctx, self._stream()), "clear_errors")
             self._stats.err = 0
 
+    # ---- learned warm start (no reference counterpart) ----------------------
+    @property
+    def log_new_contacts(self) -> bool:
+        """Queue the 20 features (and group id) of every new contact each
+        substep; new_contact_log() reads the queue of the last substep."""
+        return self._log_new
+
+    @log_new_contacts.setter
+    def log_new_contacts(self, on: bool) -> None:
+        self._log_new = bool(on)
+        if self._arena is not None and self._log_new and self._arena.dims.new_cap == 0:
+            self._dirty = True  # re-flush with a queue (keeps bodies, empties the contact cache)
+
+    @property
+    def warm_start(self):
+        """The learned warm-start model (avbd_b200.learned.WarmStartMLP) or None."""
+        return self._mlp
+
+    @warm_start.setter
+    def warm_start(self, model) -> None:
+        had = self._mlp is not None
+        self._mlp = model
+        if self._arena is None:
+            return
+        if (model is not None) != had or (model is not None and self._arena.dims.new_cap == 0):
+            self._dirty = True
+        elif model is not None:
+            with torch.cuda.stream(self._cuda_stream):
+                self._arena.view("MLP_W", torch.float32, (model.n_floats,)).copy_(model.packed(self.device))
+
+    @_on_stream
+    def new_contact_log(self):
+        """(features [n, 20] float32, group ids [n] int32) of the new contacts
+        queued by the last substep (queue order is not deterministic)."""
+        if self._arena is None or self._arena.dims.new_cap == 0:
+            return np.zeros((0, _lib.MLP_IN), np.float32), np.zeros(0, np.int32)
+        n = min(int(self._stats.n_new_logged), self._arena.dims.new_cap)
+        cap = self._arena.dims.new_cap
+        feat = self._arena.view("MLP_FEAT", torch.float32, (cap, _lib.MLP_IN))[:n].cpu().numpy()
+        gid = self._arena.view("NEW_LIST", torch.int32, (cap,))[:n].cpu().numpy()
+        return feat, gid
+
+    @_on_stream
+    def group_state(self, gid):
+        """(lambda [n, 4], penalty [n, 4]) of contact groups `gid` (the state
+        the contact cache stores for them after this substep)."""
+        idx = torch.as_tensor(np.asarray(gid, np.int64), device=self.device)
+        return self._g_lam[idx].cpu().numpy(), self._g_pen[idx].cpu().numpy()
+
+    @_on_stream
+    def clear_contact_cache(self) -> None:
+        """Empties the contact cache: every contact of the next substep is new."""
+        self._flush()
+        if self._ctx is not None:
+            _lib.check(_lib.load().avbd_cache_load(self._ctx, 0, None, None, self._stream()), "cache clear")
+
     def stats(self) -> dict:
         s = self._stats
-        return {k: getattr(s, k) for k, _ in _lib.AvbdStats._fields_ if k != "viol"}
+        return {k: getattr(s, k) for k, _ in _lib.AvbdStats._fields_ if k not in ("viol", "viol_contact")}
 
     def violation_history(self) -> np.ndarray:
+        """Max constraint violation after each iteration of the last substep
+        (record_violation): max(0, -C) of contact normals, |C| of pins, C
+        relative to alpha*C0 for hard rows."""
         s = self._stats
         return np.array(s.viol[: s.n_viol], np.float64)
+
+    def contact_violation_history(self) -> np.ndarray:
+        """Mean violation of the box-box contacts after each iteration of the
+        last substep (record_violation)."""
+        s = self._stats
+        return np.array(s.viol_contact[: s.n_viol], np.float64)
 
     @property
     def n_active_rows(self) -> torch.Tensor:

@@ -53,7 +53,9 @@ typedef struct AvbdDims {
   int dyn_row_cap;     /* dynamic contact rows (reference n_dyn_capacity) */
   int dyn_group_cap;   /* dynamic contact groups (<= dyn_row_cap) */
   int hash_cap;        /* contact-cache slots, power of two */
-  int mlp_floats;      /* learned warm-start weights (0 = none) */
+  int mlp_floats;      /* learned warm-start weights: 0 or AVBD_MLP_FLOATS */
+  int new_cap;         /* new contacts queued per substep for the learned
+                          warm start / training log (0 = none) */
 } AvbdDims;
 
 /* Scalars of Solver6DOF.__init__ (solver_6dof.py:180-201). */
@@ -78,6 +80,7 @@ typedef struct AvbdParams {
   int debug_skip_arrive; /* test hook: block 0 skips one barrier arrival */
   int blocks_per_sm;   /* persistent grid: CTAs per SM (0 = occupancy max) */
   int timing;          /* stamp the persistent kernel's phase boundaries */
+  int log_new_contacts;/* queue the features of every new contact (training) */
 } AvbdParams;
 
 typedef struct AvbdStats {
@@ -89,6 +92,10 @@ typedef struct AvbdStats {
   int capture_err;  /* 1000 * collision capture error + solve capture error */
   long long kernels_launched; /* kernels enqueued by this context so far */
   float viol[64];
+  int n_new_logged;   /* new contacts queued last substep (may exceed new_cap) */
+  int n_mlp_applied;  /* of those, warm-started by the MLP */
+  int n_mlp_fallback; /* of those, sent back to the zero start */
+  float viol_contact[64]; /* per-iteration mean violation of box-box contacts */
 } AvbdStats;
 
 typedef struct AvbdCtx AvbdCtx;
@@ -156,6 +163,62 @@ int avbd_read_phase_marks(AvbdCtx* ctx, long long* t_ns, int* phase, int cap, vo
  * array: calls that overlap on the GPU race, so serialise them.  `in` and
  * `out` are device pointers; asynchronous on `stream`. */
 int avbd_exclusive_scan_noalloc(const int* in, int* out, int n, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Learned warm start.  No counterpart in the reference: it replaces the
+ * cache-miss defaults of gpu_pool_emit_rows (kernels_6dof.py:2864-2879:
+ * lambda 0, penalties (1e6, 1, 1)) with a prediction, which the prelude
+ * (kernels_6dof.py:1596-1609) then treats like a cached value.
+ *
+ * Network: 20 features -> 64 -> 64 -> 4, SiLU, FP32 master weights.
+ * Features of a new contact (reference body a, incident body b):
+ *   0-2  contact normal in a's body frame     3  penetration depth (m)
+ *   4-6  relative contact-point velocity (a - b) along (t, b, n)
+ *   7-8  inverse masses of a, b               9-10  n^T I^-1 n of a, b
+ *   11   static friction mu_s                 12  dynamic friction mu
+ *   13-19  one-hot SAT axis class of the pair (A = the lower body index):
+ *          face of A (x, y, z), face of B (x, y, z), edge-edge.
+ * Outputs (targets, before the stored normalisation):
+ *   y0 = log1p(-lambda_n), y1 = lambda_t1 / (|lambda_n| + 1),
+ *   y2 = lambda_t2 / (|lambda_n| + 1), y3 = log(k_n).
+ *
+ * AVBD_MLP_PARAMS master parameters, in order: W1[64][20], b1[64],
+ * W2[64][64], b2[64], W3[4][64], b3[4] (row-major, out x in).
+ * AVBD_MLP_FLOATS packed inference block (floats; bf16 pairs in uint32):
+ *   [0,32) feature mean  [32,64) 1/feature std  [64,68) target mean
+ *   [68] lambda scale zeta (the decoded forces are multiplied by it)
+ *   [72,80) target std  [80,144) b1  [144,208) b2  [208,216) b3
+ *   [216,1240) W1 bf16 [64][32]  [1240,3288) W2 bf16 [64][64]
+ *   [3288,3544) W3 bf16 [8][64]  (zero padded).
+ */
+#define AVBD_MLP_IN 20
+#define AVBD_MLP_OUT 4
+#define AVBD_MLP_PARAMS 5764
+#define AVBD_MLP_FLOATS 3544
+
+/* Builds the packed inference block from master parameters `theta` and the
+ * normalisation `norm` (feature mean[20], feature std[20], target mean[4],
+ * target std[4], lambda scale zeta[1]: 49 floats).  Device pointers. */
+int avbd_mlp_pack(const float* theta, const float* norm, float* packed, void* stream);
+
+/* BF16 tensor-core forward (the solver's path) of n raw feature rows:
+ * out = n x 4 targets (denormalised).  Device pointers. */
+int avbd_mlp_infer(const float* packed, const float* feat, int n, float* out, void* stream);
+
+/* Bytes of scratch avbd_mlp_loss_grad needs for n samples. */
+size_t avbd_mlp_scratch_bytes(int n);
+
+/* FP32 loss and gradient over n normalised samples x (n x 20) with targets
+ * y (n x 4): loss = mean over samples of the summed squared error of the 4
+ * outputs; grad has AVBD_MLP_PARAMS floats.  Deterministic (fixed reduction
+ * order).  Device pointers; `loss` receives one float. */
+int avbd_mlp_loss_grad(const float* theta, const float* x, const float* y, int n, float* grad, float* loss,
+                       void* scratch, size_t scratch_bytes, void* stream);
+
+/* One Adam step (bias-corrected, step number t >= 1) on AVBD_MLP_PARAMS
+ * parameters with moment buffers m, v. */
+int avbd_mlp_adam(float* theta, const float* grad, float* m, float* v, int t, float lr, float beta1, float beta2,
+                  float eps, void* stream);
 
 /* Last error text of this thread. */
 const char* avbd_last_error(void);

@@ -923,7 +923,9 @@ template <class R> struct Sim {
     }
   }
 
-  // Max constraint violation: max(0,-C) for unilateral rows, |C| for pins.
+  // Max constraint violation: max(0,-C) for unilateral rows, |C| for pins,
+  // C being the value the dual update drives (kernels_6dof.py:1484-1507):
+  // hard rows are measured relative to their stored alpha*C0.
   double violation() const {
     double mx = 0;
     for (int j = 0; j < n_rows; ++j) {
@@ -931,6 +933,7 @@ template <class R> struct Sim {
       int t = type[j];
       if (t == TANGENT) continue;
       double C = (double)eval_C(j, x, q);
+      if (stiff[j] >= FINF) C -= (double)ac0[j];
       double vv = t == PIN ? std::fabs(C) : std::max(0.0, -C);
       mx = std::max(mx, vv);
     }

@@ -1,0 +1,222 @@
+"""Learned warm start on the GPU, checked against the numpy restatement
+(oracle/mlp_ref.py): the BF16 tensor-core inference, the FP32 loss/gradient
+and Adam kernels, the packed layout, and the features the emission logs for
+new contacts."""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp_ref as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _lib():
+    from avbd_b200 import _lib as L
+    return L, L.load()
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _problem(n, seed=0):
+    rng = np.random.default_rng(seed)
+    th = (rng.normal(0, 0.25, M.N_PARAMS)).astype(np.float32)
+    feat = rng.normal(0, 1, (n, 20)).astype(np.float32)
+    feat[:, 13:] = 0.0
+    feat[np.arange(n), 13 + rng.integers(0, 7, n)] = 1.0
+    feat[:, 3] = np.abs(feat[:, 3]) * 1e-3
+    norm = np.concatenate([rng.normal(0, 0.2, 20), rng.uniform(0.5, 2.0, 20), rng.normal(0, 1, 4),
+                           rng.uniform(0.5, 3.0, 4), [0.8]]).astype(np.float32)
+    return th, feat, norm
+
+
+def test_pack_is_bit_exact():
+    Lm, L = _lib()
+    th, _, norm = _problem(1)
+    dth, dn = torch.as_tensor(th, device="cuda"), torch.as_tensor(norm, device="cuda")
+    out = torch.empty(M.N_FLOATS, dtype=torch.float32, device="cuda")
+    assert L.avbd_mlp_pack(_p(dth), _p(dn), _p(out), None) == 0
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), M.pack(th, norm).view(np.uint32))
+
+
+@pytest.mark.parametrize("n", [1, 16, 1000, 40001])
+def test_infer_matches_bf16_restatement(n):
+    from avbd_b200.learned import WarmStartMLP
+    th, feat, norm = _problem(n, seed=n)
+    got = WarmStartMLP(theta=th, norm=norm).infer(feat)
+    ref = M.infer_bf16(M.pack(th, norm), feat)
+    err = np.abs(got - ref) / (1.0 + np.abs(ref))
+    # BF16 operands are identical; only the FP32 accumulation order differs,
+    # which can move an activation across a BF16 rounding boundary.
+    assert err.max() < 2e-2, err.max()
+    assert np.median(err) < 2e-4, np.median(err)
+
+
+def test_infer_tensor_core_vs_fp32_network():
+    """The BF16 path stays close to the FP32 network it was trained as."""
+    from avbd_b200.learned import WarmStartMLP
+    th, feat, norm = _problem(4096, seed=5)
+    got = WarmStartMLP(theta=th, norm=norm).infer(feat)
+    xn = (feat - norm[:20]) / norm[20:40]
+    ref = M.forward(th, xn)[-1] * norm[44:48] + norm[40:44]
+    scale = np.abs(ref).max(0)
+    assert (np.abs(got - ref).max(0) / scale).max() < 0.05
+
+
+@pytest.mark.parametrize("n", [1, 37, 5000])
+def test_loss_grad_matches_fp64_restatement(n):
+    Lm, L = _lib()
+    th, x, _ = _problem(n, seed=7)
+    y = np.random.default_rng(8).normal(0, 1, (n, 4)).astype(np.float32)
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device="cuda")
+    dth, dx, dy = d(th), d(x), d(y)
+    g = torch.zeros(M.N_PARAMS, dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    nb = int(L.avbd_mlp_scratch_bytes(n))
+    scratch = torch.empty(nb // 4 + 1, dtype=torch.float32, device="cuda")
+    assert L.avbd_mlp_loss_grad(_p(dth), _p(dx), _p(dy), n, _p(g), _p(loss), _p(scratch), nb, None) == 0
+    torch.cuda.synchronize()
+    ref_loss, ref_g = M.loss_grad(th, x, y)
+    assert abs(loss.item() - ref_loss) <= 1e-4 * ref_loss
+    gg = g.cpu().numpy()
+    np.testing.assert_allclose(gg, ref_g, rtol=1e-3, atol=1e-5 * np.abs(ref_g).max())
+    # deterministic: a second call is bit-identical
+    g2 = torch.zeros_like(g)
+    assert L.avbd_mlp_loss_grad(_p(dth), _p(dx), _p(dy), n, _p(g2), _p(loss), _p(scratch), nb, None) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(g, g2)
+
+
+def test_loss_grad_rejects_small_scratch():
+    Lm, L = _lib()
+    t = torch.zeros(16, device="cuda")
+    r = L.avbd_mlp_loss_grad(_p(t), _p(t), _p(t), 1000, _p(t), _p(t), _p(t), 8, None)
+    assert r < 0 and b"scratch" in L.avbd_last_error()
+
+
+def test_adam_matches_restatement():
+    Lm, L = _lib()
+    rng = np.random.default_rng(11)
+    th, g = rng.normal(0, 1, M.N_PARAMS).astype(np.float32), rng.normal(0, 1, M.N_PARAMS).astype(np.float32)
+    m, v = rng.normal(0, 0.1, M.N_PARAMS).astype(np.float32), rng.uniform(0, 0.1, M.N_PARAMS).astype(np.float32)
+    d = lambda a: torch.as_tensor(a.copy(), device="cuda")
+    dth, dg, dm, dv = d(th), d(g), d(m), d(v)
+    assert L.avbd_mlp_adam(_p(dth), _p(dg), _p(dm), _p(dv), 3, C.c_float(1e-3), C.c_float(0.9), C.c_float(0.999),
+                           C.c_float(1e-8), None) == 0
+    torch.cuda.synchronize()
+    rth, rm, rv = M.adam(th, g, m, v, 3, 1e-3, 0.9, 0.999, 1e-8)
+    # FP32 on both sides; the device contracts a*b+c into FMAs (a few ulp)
+    np.testing.assert_allclose(dm.cpu().numpy(), rm, rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(dv.cpu().numpy(), rv, rtol=1e-4, atol=1e-9)
+    np.testing.assert_allclose(dth.cpu().numpy(), rth, rtol=1e-5, atol=1e-6)
+
+
+def test_fit_learns_a_smooth_map():
+    from avbd_b200.learned import WarmStartMLP
+    rng = np.random.default_rng(2)
+    x = rng.normal(0, 1, (20000, 20)).astype(np.float32)
+    y = np.stack([np.tanh(x[:, 0] + 0.5 * x[:, 1]), x[:, 2] * x[:, 3], np.sin(x[:, 4]), x[:, 5] ** 2], 1)
+    model = WarmStartMLP(seed=0)
+    hist = model.fit(x, y, epochs=25, batch=1024, lr=3e-3)
+    assert hist[-1] < 0.1 * hist[0], hist
+    pred = model.infer(x[:2000])
+    assert np.mean((pred - y[:2000]) ** 2) < 0.1 * np.var(y[:2000], axis=0).sum()
+
+
+def _mlp_scene(seed=0):
+    from avbd_b200 import Solver6DOF, scenes
+    s = Solver6DOF(dt=1 / 60, iterations=10, substeps=4, friction_static_mult=1.25, coloring_mode="jones_plassmann")
+    scenes.pile(s, nx=6, nz=6, ny=4, seed=seed, pin_every=0)
+    return s
+
+
+def test_feature_log_matches_restatement():
+    from avbd_b200.solver import box_inertia_local
+    s = _mlp_scene()
+    for _ in range(40):
+        s.step()
+    s.log_new_contacts = True
+    sd = s.state_dict()
+    s.load_state_dict(sd)
+    s.clear_contact_cache()
+    s.substep()
+    st = s.stats()
+    feat, gid = s.new_contact_log()
+    assert st["n_new_logged"] == st["n_dyn_groups"] > 20  # every contact is new after the clear
+    assert len(gid) == st["n_new_logged"] and len(set(gid.tolist())) == len(gid)
+    pairs = s.pairs()
+    sat_of = {(int(a), int(b)): int(k) for a, b, k in zip(pairs["a"], pairs["b"], pairs["sat_idx"])}
+    body = s._g_body[gid.tolist()].cpu().numpy()
+    offa = s._g_offa[gid.tolist()].cpu().numpy()
+    offb = s._g_offb[gid.tolist()].cpu().numpy()
+    nrm = s._g_n[gid.tolist()].cpu().numpy()
+    mat = s._g_mat[gid.tolist()].cpu().numpy()
+    mass = np.array(s._mass)
+    inert = [np.diag(box_inertia_local(m, *h)) for m, h in zip(s._mass, s._half_extents)]
+    for k in range(len(gid)):
+        a, b = int(body[k, 0]), int(body[k, 1])
+        sat = sat_of[(min(a, b), max(a, b))]
+        ref = M.contact_features(sd["x"][a], sd["q"][a], sd["v"][a], sd["w"][a], mass[a], inert[a],
+                                 sd["x"][b], sd["q"][b], sd["v"][b], sd["w"][b], mass[b], inert[b],
+                                 nrm[k, :3], offa[k, :3], offb[k, :3], offa[k, 3], mat[k, 1], mat[k, 0], sat)
+        np.testing.assert_allclose(feat[k], ref, rtol=2e-4, atol=2e-5, err_msg=f"contact {k}")
+
+
+def test_warm_start_applies_and_is_deterministic():
+    from avbd_b200.learned import WarmStartMLP
+    s = _mlp_scene(1)
+    for _ in range(40):
+        s.step()
+    # a model trained on nothing still runs the path: predictions pass or fall back
+    model = WarmStartMLP(seed=3)
+    s.warm_start = model
+    sd = s.state_dict()
+    outs = []
+    for _ in range(2):
+        s.load_state_dict(sd)
+        s.clear_contact_cache()
+        s.substep()
+        st = s.stats()
+        assert st["n_mlp_applied"] + st["n_mlp_fallback"] == st["n_new_logged"] == st["n_dyn_groups"]
+        outs.append(s.state_dict())
+    np.testing.assert_array_equal(outs[0]["x"], outs[1]["x"])
+    # disabled: the zero start, bit-identical to a solver without a model
+    model.enabled = False
+    s.load_state_dict(sd)
+    s.clear_contact_cache()
+    s.substep()
+    assert s.stats()["n_mlp_applied"] == 0
+    x_off = s.state_dict()["x"]
+    s2 = _mlp_scene(1)
+    for _ in range(40):
+        s2.step()
+    s2.load_state_dict(sd)
+    s2.clear_contact_cache()
+    s2.substep()
+    np.testing.assert_array_equal(x_off, s2.state_dict()["x"])
+
+
+@pytest.mark.parametrize("seed,frame", [(1000, 240), (1001, 400)])
+def test_shipped_warm_start_cuts_iterations(seed, frame):
+    """The shipped weights (trained on seeds 0..23) on held-out piles: with
+    the contact cache emptied, the learned start reaches a mean box-box
+    contact violation of 1e-5 m in clearly fewer iterations than the zero
+    start of the reference."""
+    from avbd_b200.learned import WarmStartMLP, cold_start_violation, iterations_to
+    from avbd_b200.train_warm_start import make_pile, snapshots
+    model = WarmStartMLP.load()
+    s = make_pile(seed, 16, 16, 8, model=model)
+    for _ in snapshots(s, [frame]):
+        pass
+    _, sp = cold_start_violation(s, 64, learned=False)
+    _, sl = cold_start_violation(s, 64, learned=True)
+    plain = iterations_to(sp["contact_violation"], 1e-5)
+    learned = iterations_to(sl["contact_violation"], 1e-5)
+    assert sl["n_mlp_applied"] > 0.7 * sl["n_new_logged"]
+    assert learned <= 0.8 * plain, (plain, learned)
