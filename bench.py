@@ -68,19 +68,29 @@ class ClockSampler:
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+        # nvidia-smi numbers GPUs physically: map the CUDA ordinal through
+        # CUDA_VISIBLE_DEVICES (index or UUID) when it is set.
+        vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+        self.gpu = vis[gpu_index] if gpu_index < len(vis) else str(gpu_index)
         self.proc = None
         self.lines = []
 
-    def start(self):
+    def start(self, wait_s: float = 3.0):
+        """Starts sampling every 50 ms; returns once the first sample is in
+        (or after wait_s), so the timed region that follows is covered."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < wait_s:
+            time.sleep(0.01)
+        self.lines.clear()
 
     def _read(self):
         for line in self.proc.stdout:
@@ -155,6 +165,61 @@ def run_reference(args) -> None:
 
 
 # ---------------------------------------------------------------------------
+# Second half of the metric: iterations to a violation tolerance, learned vs
+# plain (zero) warm start of new contacts.
+# ---------------------------------------------------------------------------
+def warm_start_eval(seeds=(1000, 1001), frames=(240, 400), iterations=64) -> dict:
+    """Held-out 16x16x8 piles (the training distribution; training used seeds
+    0-23) with the contact cache emptied, so every contact starts new; one
+    substep of up to 64 iterations from the plain zero start and from the
+    shipped learned start.  Scores: iterations until the max violation over
+    all rows <= 1e-4 m, and until the mean violation of the box-box contacts
+    <= 1e-5 m (65 = not reached)."""
+    from avbd_b200.learned import WarmStartMLP, cold_start_violation, iterations_to
+    from avbd_b200.train_warm_start import make_pile, snapshots
+    model = WarmStartMLP.load()
+    acc = {k: [] for k in ("plain_max", "learned_max", "plain_contact", "learned_contact")}
+    applied = new = 0
+    for seed in seeds:
+        s = make_pile(seed, 16, 16, 8, model=model)
+        for _ in snapshots(s, frames):
+            for arm, learned in (("plain", False), ("learned", True)):
+                h, st = cold_start_violation(s, iterations, learned=learned)
+                acc[arm + "_max"].append(iterations_to(h, 1e-4))
+                acc[arm + "_contact"].append(iterations_to(st["contact_violation"], 1e-5))
+                if learned:
+                    applied += int(st["n_mlp_applied"])
+                    new += int(st["n_new_logged"])
+    m = {k: float(np.mean(v)) for k, v in acc.items()}
+    return {"workload": f"held-out 16x16x8 piles, seeds {list(seeds)}, frames {list(frames)}, contact cache emptied",
+            "max_iterations": iterations,
+            "iters_to_1e-4m_max_violation": {"plain": m["plain_max"], "learned": m["learned_max"],
+                                              "reduction": 1.0 - m["learned_max"] / m["plain_max"]},
+            "iters_to_1e-5m_mean_contact_violation": {"plain": m["plain_contact"], "learned": m["learned_contact"],
+                                                      "reduction": 1.0 - m["learned_contact"] / m["plain_contact"]},
+            "learned_applied_fraction": applied / max(1, new)}
+
+
+# ---------------------------------------------------------------------------
+# Multi-GPU: replicas only.  Each rank runs its own pile; the only collective
+# is this max of the per-rank timings (the job is as fast as its slowest rank).
+# ---------------------------------------------------------------------------
+def max_over_ranks(v: float, world: int, device) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_units(bodies_per_rank: int, substeps: int, steps: int, world: int) -> int:
+    """Body-substeps of the whole job: every rank steps its own replica."""
+    return bodies_per_rank * substeps * steps * world
+
+
+# ---------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------
 def run_gpu(args) -> None:
@@ -181,9 +246,12 @@ def run_gpu(args) -> None:
     for _ in range(args.settle):
         s._enqueue_step()
     s._after_frame()
+    tuned = None
+    if not (args.no_tune or args.group_size or args.blocks_per_sm):
+        from avbd_b200.autotune import autotune
+        tuned = autotune(s)  # launch shape for this scene; the scene state is restored
     for _ in range(args.warmup):
         s.step()
-    st0 = s.stats()
     stream = s._cuda_stream
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
@@ -200,6 +268,7 @@ def run_gpu(args) -> None:
     if args.profile:
         torch.cuda.profiler.start()
     k0 = s.stats()["kernels_launched"]
+    coll_list, solve_list = [], []
     for k in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -208,6 +277,10 @@ def run_gpu(args) -> None:
         with torch.cuda.stream(stream):
             ev[k][1].record(stream)
         s._after_frame()
+        # device time of the frame's last substep, per part (events on the
+        # solver's stream between the collision and solve graph launches)
+        coll_list.append(s.broadphase_ms)
+        solve_list.append(s.solve_ms)
     barrier()
     if args.profile:
         torch.cuda.profiler.stop()
@@ -215,7 +288,7 @@ def run_gpu(args) -> None:
     clk = clocks.stop()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     st = s.stats()
-    coll_ms, solve_ms = s.broadphase_ms, s.solve_ms
+    coll_ms, solve_ms = float(np.mean(coll_list)), float(np.mean(solve_list))
 
     # end to end through the public API: pinned host state in, step, poses out
     n = len(s._x)
@@ -236,21 +309,13 @@ def run_gpu(args) -> None:
     h2d = sum(int(t.numel() * 4) for t in pin_in)
     d2h = sum(int(t.numel() * 4) for t in pin_out)
 
-    def red_max(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    ms = red_max(ms)
-    e2e_s = red_max(e2e_s)
-    units = nb * PARAMS["substeps"] * args.steps * world
+    ms = max_over_ranks(ms, world, dev)
+    e2e_s = max_over_ranks(e2e_s, world, dev)
+    units = job_units(nb, PARAMS["substeps"], args.steps, world)
     value = units / (ms / 1e3)
     e2e_value = units / e2e_s
     r1 = len(s._rows)
     r2 = int(st["n_dyn_rows"])
-    pairs_c = int(st["n_dyn_groups"] > 0)  # refined below from the pair list
     p = s.pairs()
     pairs_with = int(np.sum(p["count"] > 0))
     ab = algorithmic_bytes(n, r1, r2, int(st["n_pairs"]), pairs_with, int(st["n_dyn_groups"]), PARAMS["iterations"])
@@ -279,7 +344,9 @@ def run_gpu(args) -> None:
                    "global_batch": nb * world, "seq_len": None, "parallelism": f"replicas x{world}",
                    "l2": "flushed (256 MiB write) between timed steps, outside the events",
                    "live": {"dyn_rows": r2, "static_rows": r1, "pairs": int(st["n_pairs"]),
-                            "contacts": int(st["n_dyn_groups"]), "colors": int(st["n_colors"])}},
+                            "contacts": int(st["n_dyn_groups"]), "colors": int(st["n_colors"])},
+                   "launch_shape": {"group_size": s.primal_group_size, "blocks_per_sm": s.blocks_per_sm,
+                                    "autotuned": tuned is not None}},
         "roofline": {"bound": "hbm", "kernel": "k_solve_persistent", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": ab["solve"], "launch_ms": solve_ms,
@@ -289,10 +356,15 @@ def run_gpu(args) -> None:
         "clocks": clk,
         "phase_ms_per_substep": {"collide": coll_ms, "solve": solve_ms},
     }
+    if tuned is not None:
+        line["autotune_ms_per_frame"] = {f"G{r['group_size']}x{r['blocks_per_sm']}": round(r["ms_per_frame"], 3)
+                                         for r in tuned["table"]}
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cb = cpu_rate(steps=3, warmup=1, threads=threads, settle=60)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0 and not args.no_warm_start:
+        line["warm_start"] = warm_start_eval()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -303,15 +375,17 @@ def run_gpu(args) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--settle", type=int, default=240)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="40x40x10 pile (profiling captures)")
     ap.add_argument("--profile", action="store_true", help="cudaProfilerStart/Stop around the timed steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--group-size", type=int, default=0)
-    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--group-size", type=int, default=0, help="lanes per body (0 = autotuned)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="solve CTAs per SM (0 = autotuned)")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start evaluation")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
