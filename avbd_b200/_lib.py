@@ -41,7 +41,7 @@ class AvbdStats(C.Structure):
                 ("err_where", C.c_int), ("n_cache_hits", C.c_int), ("n_new_contacts", C.c_int),
                 ("max_dg", C.c_int), ("n_viol", C.c_int), ("epoch", C.c_uint), ("graph_state", C.c_int),
                 ("capture_err", C.c_int), ("kernels_launched", C.c_longlong), ("viol", C.c_float * 64),
-                ("n_new_logged", C.c_int), ("n_mlp_applied", C.c_int), ("n_mlp_fallback", C.c_int),
+                ("n_new_logged", C.c_int), ("n_mlp_applied", C.c_int), ("n_mlp_fallback", C.c_int), ("n_mlp_reverted", C.c_int),
                 ("viol_contact", C.c_float * 64)]
 
 # Learned warm-start network sizes (avbd6.h AVBD_MLP_*).

@@ -431,6 +431,7 @@ int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {
   out->n_new_logged = h.n_new_logged;
   out->n_mlp_applied = h.n_mlp_applied;
   out->n_mlp_fallback = h.n_mlp_fallback;
+  out->n_mlp_reverted = h.n_mlp_reverted;
   for (int k = 0; k < 64; ++k) out->viol_contact[k] = h.vc_cnt[k] > 0 ? h.vc_sum[k] / (float)h.vc_cnt[k] : 0.0f;
   for (int k = 0; k < 64; ++k) {
     unsigned b = h.viol_bits[k];

@@ -44,6 +44,7 @@ __global__ void k_begin_substep(const __grid_constant__ Dev d) {
     c->n_new_logged = 0;
     c->n_mlp_applied = 0;
     c->n_mlp_fallback = 0;
+    c->n_mlp_reverted = 0;
     c->max_dg = 0;
     c->n_viol = 0;
     c->bar_count = 0;
@@ -808,6 +809,7 @@ __global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_g
         d.g_mat[g] = make_float4(mu, mus, __int_as_float(0x7f800000), __int_as_float(0x7f800000));
         float4 s0 = make_float4(0.0f, 0.0f, 0.0f, PEN_MIN);
         float4 s1 = make_float4(PEN_MIN_T, PEN_MIN_T, 0.0f, 0.0f);
+        bool queued = false;
         int slot = cache_find(d, cache_key(ab.x, ab.y, c), tag);
         if (slot >= 0) {
           s0 = d.h_s0[slot];
@@ -815,9 +817,11 @@ __global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_g
           ++hits;
         } else if (d.prm->mlp_on || d.prm->log_new) {
           // A new contact: queue it (with its features) for the learned
-          // warm start or for the training log.
+          // warm start (its prelude then runs in that phase) or for the
+          // training log.
           int k = atomicAdd(&d.ctr->n_new_logged, 1);
           if (k < d.new_cap) {
+            queued = d.prm->mlp_on != 0;
             d.new_list[k] = g;
             contact_features(d, ref, inc, nn, d.pair_off[8 * p + c], d.pair_off[8 * p + 4 + c], (info >> 1) & 31, mu,
                              mus, d.mlp_feat + (size_t)MLP_IN * k);
@@ -829,6 +833,7 @@ __global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_g
         int act = rpc == 3 ? (FL_ACT0 | FL_ACT1 | FL_ACT2) : FL_ACT0;
         int fl = act;
         if (rpc == 3) fl |= ((int)s1.z != 0 ? FL_WAST : 0) | ((int)s1.w != 0 ? FL_WASB : 0);
+        if (queued) fl |= FL_NEW;
         d.g_flags[g] = fl;
         ++kept;
       }
@@ -922,7 +927,6 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
   k_dg_fill<<<grid, 256, 0, st>>>(d);
   k_dg_sort<<<grid, 128, 0, st>>>(d);
   g_kernel_launches += 13;  // the direct launches above (scans and sort count themselves)
-  if (dims.mlp_floats > 0 && dims.new_cap > 0) launch_mlp_warm(d, st);
 }
 
 }  // namespace avbd

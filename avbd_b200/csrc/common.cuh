@@ -30,8 +30,14 @@ __host__ __device__ inline int make_meta(int kind, int three, int hard, int cidx
 }
 // g_flags bit layout: bits 0-2 row active, bit 3 normal row was_static,
 // bits 4/5 the friction rows' own was_static (carried to the cache), bit 6:
-// body_b owns the group (runs its dual update; else body_a).
-enum : int { FL_ACT0 = 1, FL_ACT1 = 2, FL_ACT2 = 4, FL_WAS = 8, FL_WAST = 16, FL_WASB = 32, FL_OWNB = 64 };
+// body_b owns the group (runs its dual update; else body_a), bit 7: a new
+// contact whose prelude runs in the learned-warm-start phase, bit 8: its
+// start came from the network (checked at its first dual update), bit 9:
+// that start was reverted to the zero start.
+enum : int {
+  FL_ACT0 = 1, FL_ACT1 = 2, FL_ACT2 = 4, FL_WAS = 8, FL_WAST = 16, FL_WASB = 32, FL_OWNB = 64, FL_NEW = 128,
+  FL_LRN = 256, FL_REV = 512
+};
 
 // Penalty constants: kernels_6dof.py:50-52.
 #define PEN_MIN 1.0e6f
@@ -96,7 +102,8 @@ struct DevCounters {
   int n_new_logged;      // new contacts queued for the learned warm start / log
   int n_mlp_applied;     // new contacts that took the learned warm start
   int n_mlp_fallback;    // new contacts that fell back to the zero start
-  int pad[11];
+  int n_mlp_reverted;    // learned starts reverted at their first dual (residual rose)
+  int pad[10];
   unsigned long long mark_t[256];  // globaltimer after each grid barrier
   int mark_id[256];                // phase id of that barrier (PH_*)
   // grid barrier state (each counter on its own 128-byte line): blocks

@@ -24,7 +24,5 @@ void launch_reset(Dev& d, cudaStream_t st);
 int count_conflicts(Dev& d, cudaStream_t st);
 void launch_hash_scrub(Dev& d, cudaStream_t st);
 void launch_cache_load(Dev& d, int n, const int* abc, const float* st, cudaStream_t s);
-// Learned warm start of the new contacts queued by the emission.
-void launch_mlp_warm(const Dev& d, cudaStream_t st);
 
 }  // namespace avbd

@@ -3,17 +3,18 @@
 // contact would have had, in place of the cache-miss defaults of the
 // emission (kernels_6dof.py:2864-2879).  No counterpart in the reference.
 //
-//  * Inference (the solver's path): one warp per 16-contact tile on the
-//    tensor cores, mma.sync.m16n8k16 with BF16 operands and FP32
-//    accumulation; the packed weights are staged once per block in shared
-//    memory; hidden activations stay in registers (an m16n8 accumulator
-//    tile is, lane for lane, the A fragment of the next layer's m16n8k16).
+//  * Inference (mlp.cuh; the solver runs it inside the prelude phase of
+//    the solve kernel): one warp per 16-contact tile on the tensor cores,
+//    mma.sync.m16n8k16 with BF16 operands and FP32 accumulation; the packed
+//    weights are staged once per block in shared memory; hidden activations
+//    stay in registers (an m16n8 accumulator tile is, lane for lane, the A
+//    fragment of the next layer's m16n8k16).  avbd_mlp_infer runs the same
+//    tile code stand-alone.
 //  * Training: FP32 forward/backward over 32-sample tiles in shared memory,
 //    per-block gradient partials in registers, a fixed-order reduction
 //    across blocks (bit-reproducible), and a bias-corrected Adam step.
-#include <cuda_bf16.h>
-
 #include "kernels.cuh"
+#include "mlp.cuh"
 
 namespace avbd {
 
@@ -21,189 +22,6 @@ namespace {
 
 constexpr int P_W1 = 0, P_B1 = 1280, P_W2 = 1344, P_B2 = 5440, P_W3 = 5504, P_B3 = 5760;
 static_assert(P_B3 + 4 == AVBD_MLP_PARAMS, "master parameter count");
-
-__device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
-  __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);  // .x (low half) = lo
-  return *reinterpret_cast<uint32_t*>(&h);
-}
-
-__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
-
-// Copies the packed block into shared memory (whole block participates).
-__device__ __forceinline__ void stage_weights(const float* __restrict__ w, float* sw) {
-  for (int k = threadIdx.x; k < AVBD_MLP_FLOATS; k += blockDim.x) sw[k] = w[k];
-  __syncthreads();
-}
-
-// Forward pass of one 16-row tile by one warp.  `feat` points at row 0 of
-// the tile (MLP_IN raw floats per row), `rows` valid rows (1..16).  On
-// return lanes with (lane & 3) < 2 hold the denormalised outputs of rows
-// g = lane >> 2 and g + 8 at columns 2t, 2t+1 (t = lane & 3): y[0..1] for
-// row g, y[2..3] for row g + 8.
-__device__ __forceinline__ void mlp_tile(const float* sw, const float* __restrict__ feat, int rows, float (&y)[4]) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const uint32_t* W1 = reinterpret_cast<const uint32_t*>(sw + MLPO_W1);
-  const uint32_t* W2 = reinterpret_cast<const uint32_t*>(sw + MLPO_W2);
-  const uint32_t* W3 = reinterpret_cast<const uint32_t*>(sw + MLPO_W3);
-  // Layer-1 A fragments: rows g and g+8, columns {2t, 2t+1, 2t+8, 2t+9} of
-  // both 16-wide k-steps; normalised, zero beyond MLP_IN and beyond `rows`.
-  uint32_t a[2][4];
-#pragma unroll
-  for (int kk = 0; kk < 2; ++kk) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {      // h: column half (+0 / +8)
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {    // r: row g / g+8
-        int row = g + 8 * r;
-        int col = 16 * kk + 8 * h + 2 * t;
-        float v0 = 0.0f, v1 = 0.0f;
-        if (row < rows) {
-          if (col < MLP_IN) v0 = (feat[row * MLP_IN + col] - sw[MLPO_FMEAN + col]) * sw[MLPO_FISTD + col];
-          if (col + 1 < MLP_IN)
-            v1 = (feat[row * MLP_IN + col + 1] - sw[MLPO_FMEAN + col + 1]) * sw[MLPO_FISTD + col + 1];
-        }
-        a[kk][2 * h + r] = bf16x2(v0, v1);
-      }
-    }
-  }
-  // Layer 1: 8 n-tiles of 8 hidden units.
-  float h1[8][4];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    float b0 = sw[MLPO_B1 + 8 * j + 2 * t], b1 = sw[MLPO_B1 + 8 * j + 2 * t + 1];
-    h1[j][0] = b0; h1[j][1] = b1; h1[j][2] = b0; h1[j][3] = b1;
-#pragma unroll
-    for (int kk = 0; kk < 2; ++kk) {
-      const uint32_t* wr = W1 + (8 * j + g) * 16 + 8 * kk + t;
-      mma_bf16(h1[j], a[kk][0], a[kk][1], a[kk][2], a[kk][3], wr[0], wr[4]);
-    }
-#pragma unroll
-    for (int e = 0; e < 4; ++e) h1[j][e] = silu(h1[j][e]);
-  }
-  // Layer 2: the accumulator tiles 2kk, 2kk+1 are the A fragment of k-step kk.
-  float h2[8][4];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    float b0 = sw[MLPO_B2 + 8 * j + 2 * t], b1 = sw[MLPO_B2 + 8 * j + 2 * t + 1];
-    h2[j][0] = b0; h2[j][1] = b1; h2[j][2] = b0; h2[j][3] = b1;
-  }
-#pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
-    uint32_t a0 = bf16x2(h1[2 * kk][0], h1[2 * kk][1]), a1 = bf16x2(h1[2 * kk][2], h1[2 * kk][3]);
-    uint32_t a2 = bf16x2(h1[2 * kk + 1][0], h1[2 * kk + 1][1]), a3 = bf16x2(h1[2 * kk + 1][2], h1[2 * kk + 1][3]);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const uint32_t* wr = W2 + (8 * j + g) * 32 + 8 * kk + t;
-      mma_bf16(h2[j], a0, a1, a2, a3, wr[0], wr[4]);
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < 8; ++j)
-#pragma unroll
-    for (int e = 0; e < 4; ++e) h2[j][e] = silu(h2[j][e]);
-  // Layer 3: one n-tile (outputs 0..3 used, 4..7 zero weights).
-  float o[4];
-  {
-    float b0 = sw[MLPO_B3 + 2 * t], b1 = sw[MLPO_B3 + 2 * t + 1];
-    o[0] = b0; o[1] = b1; o[2] = b0; o[3] = b1;
-  }
-#pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
-    uint32_t a0 = bf16x2(h2[2 * kk][0], h2[2 * kk][1]), a1 = bf16x2(h2[2 * kk][2], h2[2 * kk][3]);
-    uint32_t a2 = bf16x2(h2[2 * kk + 1][0], h2[2 * kk + 1][1]), a3 = bf16x2(h2[2 * kk + 1][2], h2[2 * kk + 1][3]);
-    const uint32_t* wr = W3 + g * 32 + 8 * kk + t;
-    mma_bf16(o, a0, a1, a2, a3, wr[0], wr[4]);
-  }
-  int c = 2 * (t & 1);  // output columns of this lane (t = 0: 0,1; t = 1: 2,3)
-  float m0 = sw[MLPO_OMEAN + c], m1 = sw[MLPO_OMEAN + c + 1];
-  float s0 = sw[MLPO_OSTD + c], s1 = sw[MLPO_OSTD + c + 1];
-  y[0] = o[0] * s0 + m0;
-  y[1] = o[1] * s1 + m1;
-  y[2] = o[2] * s0 + m0;
-  y[3] = o[3] * s1 + m1;
-}
-
-// Gathers the 4 outputs of rows g and g+8 into lane 4g: out_g[4], out_g8[4].
-__device__ __forceinline__ void gather_rows(const float (&y)[4], float (&og)[4], float (&og8)[4]) {
-  float n0 = __shfl_down_sync(0xffffffffu, y[0], 1), n1 = __shfl_down_sync(0xffffffffu, y[1], 1);
-  float n2 = __shfl_down_sync(0xffffffffu, y[2], 1), n3 = __shfl_down_sync(0xffffffffu, y[3], 1);
-  og[0] = y[0]; og[1] = y[1]; og[2] = n0; og[3] = n1;
-  og8[0] = y[2]; og8[1] = y[3]; og8[2] = n2; og8[3] = n3;
-}
-
-// Targets -> warm-start state (forces scaled by zeta).  Returns false when
-// the contact must keep the zero start: separated (depth <= 0), non-finite,
-// or a predicted friction force outside the static cone
-// (|lambda_t| > mu_s |lambda_n|).
-__device__ __forceinline__ bool decode_start(const float (&y)[4], float depth, float mus, float zeta, float4& lam,
-                                             float& kn) {
-  float ln0 = -expm1f(fmaxf(y[0], 0.0f));
-  float sc = fabsf(ln0) + 1.0f;
-  float ln = zeta * ln0;
-  float lt = zeta * (y[1] * sc), lb = zeta * (y[2] * sc);
-  kn = fminf(fmaxf(expf(y[3]), PEN_MIN), PEN_MAX);
-  lam = make_float4(ln, lt, lb, 0.0f);
-  if (!(depth > 0.0f)) return false;
-  if (!isfinite(ln) || !isfinite(lt) || !isfinite(lb) || !isfinite(kn)) return false;
-  if (sqrtf(lt * lt + lb * lb) > mus * fabsf(ln)) return false;
-  return true;
-}
-
-__global__ void __launch_bounds__(128) k_mlp_warm(const __grid_constant__ Dev d) {
-  __shared__ float sw[AVBD_MLP_FLOATS];
-  if (!d.prm->mlp_on) return;
-  int n = min(d.ctr->n_new_logged, d.new_cap);
-  if (n <= 0) return;
-  stage_weights(d.mlp_w, sw);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  int applied = 0, fallback = 0;
-  for (int tile = blockIdx.x * nw + warp; tile * 16 < n; tile += gridDim.x * nw) {
-    int r0 = tile * 16, rows = min(16, n - r0);
-    float y[4], og[4], og8[4];
-    mlp_tile(sw, d.mlp_feat + (size_t)r0 * MLP_IN, rows, y);
-    gather_rows(y, og, og8);
-    if ((lane & 3) == 0) {
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        int row = (lane >> 2) + 8 * r;
-        if (row >= rows) continue;
-        int k = r0 + row;
-        const float* f = d.mlp_feat + (size_t)k * MLP_IN;
-        int gid = d.new_list[k];
-        float4 lam;
-        float kn;
-        if (decode_start(r ? og8 : og, f[3], f[11], sw[MLPO_OMEAN + MLP_OUT], lam, kn)) {
-          bool three = (d.g_meta[gid] & 4) != 0;
-          if (!three) lam.y = lam.z = 0.0f;
-          d.g_lam[gid] = lam;
-          float4 pen = d.g_pen[gid];
-          pen.x = kn;
-          d.g_pen[gid] = pen;
-          ++applied;
-        } else {
-          ++fallback;
-        }
-      }
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    applied += __shfl_xor_sync(0xffffffffu, applied, o);
-    fallback += __shfl_xor_sync(0xffffffffu, fallback, o);
-  }
-  if (lane == 0) {
-    if (applied) atomicAdd(&d.ctr->n_mlp_applied, applied);
-    if (fallback) atomicAdd(&d.ctr->n_mlp_fallback, fallback);
-  }
-}
 
 __global__ void __launch_bounds__(128) k_mlp_infer(const float* __restrict__ packed, const float* __restrict__ feat,
                                                    int n, float* __restrict__ out) {
@@ -478,13 +296,6 @@ int grad_blocks(int n) {
 
 }  // namespace
 
-void launch_mlp_warm(const Dev& d, cudaStream_t st) {
-  int nblk = (d.new_cap + 63) / 64;
-  if (nblk > 4 * 148) nblk = 4 * 148;
-  if (nblk < 1) nblk = 1;
-  k_mlp_warm<<<nblk, 128, 0, st>>>(d);
-  g_kernel_launches += 1;
-}
 
 }  // namespace avbd
 

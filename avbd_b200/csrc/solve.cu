@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "mlp.cuh"
 
 namespace avbd {
 
@@ -225,6 +226,26 @@ __device__ __forceinline__ float dual_rows(int kind, int nr, bool hard, float4 m
   return vmax;
 }
 
+// The plain start as fallback when a learned start raised the residual.  At
+// the contact's first dual update (iteration 0) the normal row's opening
+// ce = C - alpha*C0 times its penalty k estimates how far the predicted
+// force lambda_p overshoots the force the contact needs (k ce ~ lambda_p -
+// lambda*).  The zero start's error is |lambda*|, so the prediction is worse
+// than no prediction when k ce > |lambda_p| / 2; such a start is dropped and
+// the group continues from lambda = 0 and the minimum penalties, as a new
+// contact of the reference would.  Clears FL_LRN either way.
+__device__ __forceinline__ void learned_check(const Dev& d, int kind, bool hard, const float* C, const float* ac,
+                                              float* lm, float* pn, int& fl) {
+  fl &= ~FL_LRN;
+  float ce = hard ? C[0] - ac[0] : C[0];
+  if (kind == KIND_BOX && lm[0] < 0.0f && ce * pn[0] > 0.5f * fabsf(lm[0])) {
+    lm[0] = lm[1] = lm[2] = 0.0f;
+    pn[0] = PEN_MIN;
+    pn[1] = pn[2] = PEN_MIN_T;
+    fl = (fl & ~FL_WAS) | FL_REV;  // counted by the cache refresh
+  }
+}
+
 // Group g's contribution to body i's system, rows in row order.  When
 // `dual` is set and body i owns g (the group's dynamic body with the lower
 // color), the previous iteration's dual update of g is applied first: both
@@ -287,6 +308,7 @@ __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3
   }
   float viol = 0.0f;
   if (dual && own) {
+    if (fl & FL_LRN) learned_check(d, kind, hard, C, ac, lm, pn, fl);
     viol = dual_rows(kind, nr, hard, mat, C, ac, d.prm->beta, lm, pn, fl);
     d.g_lam[g] = make_float4(lm[0], lm[1], lm[2], 0.0f);
     d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
@@ -604,17 +626,17 @@ __device__ __forceinline__ int n_groups_live(const Dev& d) { return d.n_sg + d.c
 // Prelude (kernels_6dof.py:1565-1672), run BEFORE predict so x/q are the
 // substep's initial pose.  Rows of a group in row order (Warp CPU order):
 // the friction check of the first tangent sees the decayed normal and first
-// tangent, and the second tangent's lambda before its own decay.
-__device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
+// tangent, and the second tangent's lambda before its own decay.  `lam`,
+// `pen` are the group's stored (cached or default) state, or the learned
+// start of a new contact.
+__device__ __forceinline__ void prelude_group(const Dev& d, int g, int fl, float4 lam, float4 pen) {
   const DevParams& P = *d.prm;
-  int ng = n_groups_live(d);
   float main_alpha = P.post_stab ? 1.0f : P.alpha;
-  for (int g = gtid; g < ng; g += gsize) {
+  {
     int meta = d.g_meta[g];
-    int fl = d.g_flags[g];
     int kind = meta_kind(meta);
     bool three = (meta & 4) != 0;
-    float4 lam = d.g_lam[g], pen = d.g_pen[g], mat = d.g_mat[g];
+    float4 mat = d.g_mat[g];
     float s = mat.z;
     bool tang = kind != KIND_PIN;  // rows 1, 2 of floor/box groups are friction rows
     float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z};
@@ -651,9 +673,76 @@ __device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
     d.g_lam[g] = make_float4(lm[0], lm[1], lm[2], 0.0f);
     d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
     d.g_ac0[g] = make_float4(a[0], a[1], a[2], 0.0f);
-    d.g_flags[g] = fl;
+    d.g_flags[g] = fl & ~FL_NEW;
   }
 }
+
+__device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
+  int ng = n_groups_live(d);
+  for (int g = gtid; g < ng; g += gsize) {
+    int fl = d.g_flags[g];
+    if (fl & FL_NEW) continue;  // its prelude runs in ph_mlp_prelude
+    prelude_group(d, g, fl, d.g_lam[g], d.g_pen[g]);
+  }
+}
+
+// Learned warm start of the new contacts the emission queued, fused with
+// their prelude: each warp runs the network on 16-contact tiles (BF16
+// mma.sync, weights staged once per block in shared memory), decodes the
+// predicted (lambda_n, lambda_t1, lambda_t2, k_n), keeps the zero start for
+// separated contacts, non-finite outputs and forces outside the static
+// friction cone, and then runs the prelude of each contact on the start it
+// chose.  Block-uniform (every thread of a block reaches the __syncthreads).
+__device__ __noinline__ void ph_mlp_prelude(const Dev& d, int gtid, int gsize) {
+  if (!d.prm->mlp_on || d.mlp_w == nullptr) return;
+  int n = min(*(volatile int*)&d.ctr->n_new_logged, d.new_cap);
+  if (n <= 0) return;
+  extern __shared__ float sw[];  // AVBD_MLP_FLOATS (dynamic shared memory of the launch)
+  stage_weights(d.mlp_w, sw);
+  const int lane = threadIdx.x & 31;
+  const float zeta = sw[MLPO_OMEAN + MLP_OUT];
+  int applied = 0, fallback = 0;
+  for (int tile = gtid >> 5; tile * 16 < n; tile += gsize >> 5) {
+    int r0 = tile * 16, rows = min(16, n - r0);
+    float y[4], og[4], og8[4];
+    mlp_tile(sw, d.mlp_feat + (size_t)r0 * MLP_IN, rows, y);
+    gather_rows(y, og, og8);
+    if ((lane & 3) == 0) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        int row = (lane >> 2) + 8 * r;
+        if (row >= rows) continue;
+        int k = r0 + row;
+        const float* f = d.mlp_feat + (size_t)k * MLP_IN;
+        int g = d.new_list[k];
+        int fl = d.g_flags[g];
+        float4 lam = d.g_lam[g], pen = d.g_pen[g];  // the zero start written by the emission
+        float4 l2;
+        float kn;
+        if (decode_start(r ? og8 : og, f[3], f[11], zeta, l2, kn)) {
+          if (!(d.g_meta[g] & 4)) l2.y = l2.z = 0.0f;
+          lam = l2;
+          pen.x = kn;
+          fl |= FL_LRN;
+          ++applied;
+        } else {
+          ++fallback;
+        }
+        prelude_group(d, g, fl, lam, pen);
+      }
+    }
+  }
+  __syncthreads();  // the shared weights are not reused before every warp is done
+  for (int o = 16; o > 0; o >>= 1) {
+    applied += __shfl_xor_sync(0xffffffffu, applied, o);
+    fallback += __shfl_xor_sync(0xffffffffu, fallback, o);
+  }
+  if (lane == 0) {
+    if (applied) atomicAdd(&d.ctr->n_mlp_applied, applied);
+    if (fallback) atomicAdd(&d.ctr->n_mlp_fallback, fallback);
+  }
+}
+
 
 // Stand-alone dual update of every group (kernels_6dof.py:1451-1548); used
 // after the last iteration when there is no post-stabilization pass to carry
@@ -672,6 +761,7 @@ __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
     float4 lam = d.g_lam[g], pen = d.g_pen[g], ac0 = d.g_ac0[g], mat = d.g_mat[g];
     GroupC cv = group_values(d, g, meta, d.x, d.q);
     float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z}, ac[3] = {ac0.x, ac0.y, ac0.z};
+    if (fl & FL_LRN) learned_check(d, kind, hard, cv.c, ac, lm, pn, fl);
     float v = dual_rows(kind, three ? 3 : 1, hard, mat, cv.c, ac, P.beta, lm, pn, fl);
     vmax = fmaxf(vmax, v);
     if (kind == KIND_BOX && (fl & FL_ACT0)) {
@@ -752,9 +842,11 @@ __device__ void ph_collect(const Dev& d, int gtid, int gsize) {
   int nd = d.ctr->n_dyn_groups;
   unsigned tag = epoch_tag(d.ctr->epoch + 1u);
   unsigned mask = (unsigned)d.hash_cap - 1u;
+  int reverted = 0;
   for (int u = gtid; u < nd; u += gsize) {
     int g = d.n_sg + u;
     int fl = d.g_flags[g];
+    if (fl & FL_REV) ++reverted;
     if (!(fl & FL_ACT0)) continue;
     int meta = d.g_meta[g];
     int2 bd = d.g_body[g];
@@ -795,6 +887,8 @@ __device__ void ph_collect(const Dev& d, int gtid, int gsize) {
     }
     if (!done) atomicOr(&d.ctr->err, ERR_HASH_FULL);
   }
+  for (int o = 16; o > 0; o >>= 1) reverted += __shfl_xor_sync(0xffffffffu, reverted, o);
+  if (lane_id() == 0 && reverted) atomicAdd(&d.ctr->n_mlp_reverted, reverted);
 }
 
 // ---------------------------------------------------------------------------
@@ -1039,6 +1133,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
   }
   ph_gate(d, gtid, gsize);
   ph_prelude(d, gtid, gsize);  // reads x/q = the initial pose; predict runs after
+  ph_mlp_prelude(d, gtid, gsize);
   SYNC(PH_GATE_PRELUDE);
   if (recolor_needed(d)) {
     bool jp = P.color_mode == 1;
@@ -1105,6 +1200,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
 // ---------------------------------------------------------------------------
 #define GS int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x
 __global__ void ks_gate_prelude(const __grid_constant__ Dev d) { GS; ph_gate(d, gtid, gsize); ph_prelude(d, gtid, gsize); }
+__global__ void ks_mlp_prelude(const __grid_constant__ Dev d) { GS; ph_mlp_prelude(d, gtid, gsize); }
 __global__ void ks_color_reset(const __grid_constant__ Dev d) {
   GS;
   if (!recolor_needed(d)) {
@@ -1175,20 +1271,28 @@ __global__ void ks_end(const __grid_constant__ Dev d) {
 
 int solve_occupancy(int block, int variant) {
   int n = 0;
-  if (variant >= 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<3>, block, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<2>, block, 0);
+  // sized with the learned warm start's shared weights, whether used or not
+  size_t smem = sizeof(float) * AVBD_MLP_FLOATS;
+  if (variant >= 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<3>, block, smem);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<2>, block, smem);
   return n;
 }
 
 cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st,
                          int variant) {
+  // dynamic shared memory: the learned warm start's weights, when present
+  size_t mlp_smem = d.mlp_w != nullptr ? sizeof(float) * AVBD_MLP_FLOATS : 0;
   if (persistent) {
     void* args[] = {(void*)&d};
     g_kernel_launches += 1;
     const void* fn = variant >= 3 ? (const void*)k_solve_persistent<3> : (const void*)k_solve_persistent<2>;
-    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, 0, st);
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, mlp_smem, st);
   }
   ks_gate_prelude<<<grid, block, 0, st>>>(d);
+  if (mlp_smem) {
+    ks_mlp_prelude<<<grid, block, mlp_smem, st>>>(d);
+    g_kernel_launches += 1;
+  }
   ks_color_reset<<<grid, block, 0, st>>>(d);
   int rounds = P.coloring_mode == 1 ? JP_ROUNDS : MAX_COLORS;
   for (int r = 0; r < rounds; ++r) {

@@ -8,8 +8,8 @@ cached state the contact would have had -- (lambda_n, lambda_t1, lambda_t2,
 k_n) -- from 20 local features, so the prelude (kernels_6dof.py:1596-1609)
 starts it near its converged force.  No counterpart exists in the reference.
 
-Everything numeric runs in libavbd6: the BF16 tensor-core inference inside
-the solver's collision pipeline (and avbd_mlp_infer), the FP32
+Everything numeric runs in libavbd6: the BF16 tensor-core inference fused
+into the prelude phase of the solve kernel (and avbd_mlp_infer), the FP32
 forward/backward (avbd_mlp_loss_grad) and Adam (avbd_mlp_adam).  Python
 holds the parameters, normalisation and the training loop.
 

@@ -326,11 +326,13 @@ def run_gpu(args) -> None:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = ab["solve"] / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    # DRAM bytes of one solve launch from an ncu capture of this workload
+    # (dram__bytes_read.sum + dram__bytes_write.sum), committed with its command
     traffic = None
     tf = os.path.join(ROOT, "profiles", "solve_traffic.json")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and not args.small:
         try:
-            traffic = json.load(open(tf)).get("bytes_per_launch_scaled")
+            traffic = json.load(open(tf)).get("bytes_per_launch")
         except Exception:
             traffic = None
     line = {

@@ -94,7 +94,11 @@ typedef struct AvbdStats {
   float viol[64];
   int n_new_logged;   /* new contacts queued last substep (may exceed new_cap) */
   int n_mlp_applied;  /* of those, warm-started by the MLP */
-  int n_mlp_fallback; /* of those, sent back to the zero start */
+  int n_mlp_fallback; /* of those, kept at the zero start (separated, non-finite,
+                         outside the static friction cone) */
+  int n_mlp_reverted; /* learned starts reset to the zero start at their first
+                         dual update because the contact separated (the
+                         predicted force raised the complementarity residual) */
   float viol_contact[64]; /* per-iteration mean violation of box-box contacts */
 } AvbdStats;
 

@@ -184,6 +184,7 @@ def test_warm_start_applies_and_is_deterministic():
         s.substep()
         st = s.stats()
         assert st["n_mlp_applied"] + st["n_mlp_fallback"] == st["n_new_logged"] == st["n_dyn_groups"]
+        assert 0 <= st["n_mlp_reverted"] <= st["n_mlp_applied"]
         outs.append(s.state_dict())
     np.testing.assert_array_equal(outs[0]["x"], outs[1]["x"])
     # disabled: the zero start, bit-identical to a solver without a model
