@@ -20,7 +20,8 @@ AVBD_ERR_BVH = 64
 class AvbdDims(C.Structure):
     _fields_ = [("n_bodies", C.c_int), ("n_static_groups", C.c_int), ("n_static_rows", C.c_int),
                 ("pair_cap", C.c_int), ("dyn_row_cap", C.c_int), ("dyn_group_cap", C.c_int),
-                ("hash_cap", C.c_int), ("mlp_floats", C.c_int), ("new_cap", C.c_int)]
+                ("hash_cap", C.c_int), ("mlp_floats", C.c_int), ("new_cap", C.c_int),
+                ("n_scenes", C.c_int)]
 
 
 class AvbdParams(C.Structure):

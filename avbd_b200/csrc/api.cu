@@ -43,7 +43,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(H_S0, 16, H) X(H_S1, 16, H) X(SCAN_PART, 4, SP) X(SORT_HIST, 4, SH) X(C_USED, 4, N) X(C_LOST, 4, N)        \
   X(C_HIST, 4, 64 * 64) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
   X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
-  X(MLP_FEAT, 4, NC * MLP_IN)
+  X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,
@@ -60,7 +60,7 @@ const char* kNames[] = {
 bool compute_layout(const AvbdDims* dm, size_t* off, size_t* total) {
   if (!dm || dm->n_bodies < 0 || dm->n_static_groups < 0 || dm->pair_cap < 0 || dm->dyn_group_cap < 0 ||
       dm->dyn_row_cap < 0 || dm->hash_cap < 1 || (dm->hash_cap & (dm->hash_cap - 1)) != 0 ||
-      (dm->mlp_floats != 0 && dm->mlp_floats != AVBD_MLP_FLOATS) || dm->new_cap < 0)
+      (dm->mlp_floats != 0 && dm->mlp_floats != AVBD_MLP_FLOATS) || dm->new_cap < 0 || dm->n_scenes < 0)
     return false;
   long long N = dm->n_bodies > 0 ? dm->n_bodies : 1;
   long long DG = dm->dyn_group_cap;
@@ -70,6 +70,7 @@ bool compute_layout(const AvbdDims* dm, size_t* off, size_t* total) {
   long long H = dm->hash_cap;
   long long M = dm->mlp_floats;
   long long NC = dm->new_cap;
+  long long NS = dm->n_scenes;
   long long nblk = (N + 2047) / 2048;
   long long SH = 256 * nblk + 1;
   long long big = P > SH ? P : SH;
@@ -200,6 +201,9 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.new_cap = dims->new_cap;
   d.new_list = PTR(int*, NEW_LIST);
   d.mlp_feat = PTR(float*, MLP_FEAT);
+  d.n_scenes = dims->n_scenes;
+  d.scene_of = dims->n_scenes > 0 ? PTR(const int*, SCENE_OF) : nullptr;
+  d.scene_tab = dims->n_scenes > 0 ? PTR(const float4*, SCENE_TAB) : nullptr;
   d.ctr = PTR(DevCounters*, COUNTERS);
 #undef PTR
   int occ = solve_occupancy(256, 2);
@@ -255,6 +259,7 @@ static void fill_devparams(AvbdCtx* c, float dt_sub) {
   q.debug_skip_arrive = P.debug_skip_arrive;
   q.mlp_on = P.mlp_warm_start && c->dims.mlp_floats > 0 && c->dims.new_cap > 0;
   q.log_new = P.log_new_contacts && c->dims.new_cap > 0;
+  q.batched = c->dims.n_scenes > 0;
   q.barrier_timeout_ns = P.debug_skip_arrive ? 200000000ull : 2000000000ull;
   q.timing = P.timing;
 }
@@ -379,9 +384,15 @@ static int run_substep(AvbdCtx* c, cudaStream_t st) {
   return AVBD_OK;
 }
 
-int avbd_substep(AvbdCtx* c, float dt, void* stream) {
-  if (!c) return fail(AVBD_E_INVALID, "null ctx");
-  cudaStream_t st = (cudaStream_t)stream;
+// Batched scenes: a frame is slots 0..substeps-1; a scene takes part in the
+// first `its substeps` slots.  The device counts slots from this reset.
+static int reset_slot(AvbdCtx* c, cudaStream_t st) {
+  if (c->dims.n_scenes <= 0) return AVBD_OK;
+  cudaError_t e = cudaMemsetAsync(&c->d.ctr->slot_next, 0, sizeof(int), st);
+  return e == cudaSuccess ? AVBD_OK : fail(AVBD_E_CUDA, "slot reset", e);
+}
+
+static int substep_impl(AvbdCtx* c, float dt, cudaStream_t st) {
   if (dt != c->cur_dt) {
     c->cur_dt = dt;
     fill_devparams(c, dt);
@@ -391,14 +402,20 @@ int avbd_substep(AvbdCtx* c, float dt, void* stream) {
   return settle_errors(run_substep(c, st), "substep");
 }
 
+int avbd_substep(AvbdCtx* c, float dt, void* stream) {
+  if (!c) return fail(AVBD_E_INVALID, "null ctx");
+  cudaStream_t st = (cudaStream_t)stream;
+  int r = reset_slot(c, st);  // batched: one substep = slot 0, every scene at its own dt
+  return r != AVBD_OK ? r : substep_impl(c, dt, st);
+}
+
 int avbd_step(AvbdCtx* c, void* stream) {
   if (!c) return fail(AVBD_E_INVALID, "null ctx");
+  cudaStream_t st = (cudaStream_t)stream;
   float dt = c->P.dt / (float)c->P.substeps;
-  for (int s = 0; s < c->P.substeps; ++s) {
-    int r = avbd_substep(c, dt, stream);
-    if (r != AVBD_OK) return r;
-  }
-  return AVBD_OK;
+  int r = reset_slot(c, st);
+  for (int s = 0; s < c->P.substeps && r == AVBD_OK; ++s) r = substep_impl(c, dt, st);
+  return r;
 }
 
 int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {

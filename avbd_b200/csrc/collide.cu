@@ -45,6 +45,8 @@ __global__ void k_begin_substep(const __grid_constant__ Dev d) {
     c->n_mlp_applied = 0;
     c->n_mlp_fallback = 0;
     c->n_mlp_reverted = 0;
+    c->slot = c->slot_next;  // substep slot within the frame (batched scenes)
+    c->slot_next = c->slot + 1;
     c->max_dg = 0;
     c->n_viol = 0;
     c->bar_count = 0;
@@ -377,6 +379,7 @@ __device__ __forceinline__ void bvh_query_upper(const Dev& d, int i, F fn) {
   int n = d.nb;
   float4 lo = d.aabb_lo[i], hi = d.aabb_hi[i];
   bool si = d.x[i].w <= 0.0f;
+  int sc = d.scene_of ? d.scene_of[i] : 0;  // batched scenes never collide with each other
   int stack[64];
   int sp = 0;
   stack[sp++] = 0;
@@ -385,7 +388,7 @@ __device__ __forceinline__ void bvh_query_upper(const Dev& d, int i, F fn) {
     if (!overlap(lo, hi, d.node_lo[node], d.node_hi[node])) continue;
     if (node >= n - 1) {
       int j = d.order[node - (n - 1)];
-      if (j > i && !(si && d.x[j].w <= 0.0f)) fn(j);
+      if (j > i && !(si && d.x[j].w <= 0.0f) && (!d.scene_of || d.scene_of[j] == sc)) fn(j);
     } else {
       if (sp + 2 > 64) {
         atomicOr(&d.ctr->err, ERR_BVH);

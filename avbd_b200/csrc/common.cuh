@@ -103,7 +103,9 @@ struct DevCounters {
   int n_mlp_applied;     // new contacts that took the learned warm start
   int n_mlp_fallback;    // new contacts that fell back to the zero start
   int n_mlp_reverted;    // learned starts reverted at their first dual (residual rose)
-  int pad[10];
+  int slot;              // substep slot within the frame (batched scenes)
+  int slot_next;         // slot of the next substep (reset by the host at frame start)
+  int pad[8];
   unsigned long long mark_t[256];  // globaltimer after each grid barrier
   int mark_id[256];                // phase id of that barrier (PH_*)
   // grid barrier state (each counter on its own 128-byte line): blocks
@@ -141,7 +143,8 @@ struct DevParams {
   unsigned long long barrier_timeout_ns;
   int timing;   // record phase timestamps in the counters
   int log_new;  // queue every new contact's features (training-data log)
-  int pad[6];
+  int batched;  // bodies belong to scenes with their own dt / iterations / substeps
+  int pad[5];
 };
 
 // Phase ids of the persistent kernel's timestamps.
@@ -196,6 +199,10 @@ struct Dev {
   int new_cap;      // capacity of the new-contact queue
   int* new_list;    // group id of each queued new contact
   float* mlp_feat;  // MLP_IN raw features of each queued new contact
+  // batched scenes (null when the arena holds one scene)
+  int n_scenes;
+  const int* scene_of;       // scene of each body
+  const float4* scene_tab;   // per scene: (substep dt, iterations, substeps per frame, 0)
   // counters
   DevCounters* ctr;
 };

@@ -454,6 +454,15 @@ __device__ __forceinline__ void prefetch_group(const Dev& d, int g, bool box) {
   }
 }
 
+// Batched scenes: a scene takes part in the first `substeps` slots of a
+// frame, at its own substep dt and iteration count (scene table entry
+// (dt, iterations, substeps, 0)).
+__device__ __forceinline__ float4 scene_entry(const Dev& d, int body) { return d.scene_tab[d.scene_of[body]]; }
+__device__ __forceinline__ bool scene_on(const Dev& d, float4 t) { return d.ctr->slot < (int)t.z; }
+__device__ __forceinline__ bool group_on(const Dev& d, int g) {
+  return !d.prm->batched || scene_on(d, scene_entry(d, d.g_body[g].x));
+}
+
 // BDF1 velocities + caps of one body (kernels_6dof.py:1871-1901).
 __device__ __forceinline__ void finalize_body(const Dev& d, int i, float dt) {
   const DevParams& P = *d.prm;
@@ -480,6 +489,7 @@ struct PassMode {
   bool dual;      // apply the previous iteration's dual update (owned groups)
   bool finalize;  // BDF1 finalize of the body before its primal
   int viol_slot;  // iteration whose violation is recorded (-1: none)
+  int it;         // pass index (batched scenes derive their own flags from it)
 };
 
 // Folds a warp's violation statistics of iteration `slot` into the
@@ -502,8 +512,10 @@ __device__ __forceinline__ void record_violation(const Dev& d, int slot, float v
 
 // Primal sweep of one color: G lanes per body, butterfly reduction of the
 // 27 accumulators, lane 0 solves (kernels_6dof.py:1149-1414, in place).
-template <int G>
+template <int G, bool B>
 __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gtid, int gsize) {
+  const int post_stab = d.prm->post_stab;
+  const int slot_now = B ? d.ctr->slot : 0;
   int cs0 = d.color_starts[c];
   int nbody = d.color_starts[c + 1] - cs0;
   int total = nbody * G;
@@ -516,6 +528,21 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
     int i = valid ? d.color_bodies[cs0 + slot] : 0;
     float4 xi4 = valid ? d.x[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     bool act = valid && xi4.w > 0.0f;
+    bool solve = act;
+    if (B) {
+      // this body's scene: its own dt; pass `it` is a main iteration while
+      // it < its, the post-stab pass (or, without it, the last dual and the
+      // finalize) at it == its, and idle beyond or in a slot it skips
+      float4 t = valid ? scene_entry(d, i) : make_float4(dt, 0.0f, 0.0f, 0.0f);
+      int its = (int)t.y;
+      dt = t.x;
+      bool on = valid && slot_now < (int)t.z && pm.it <= its;
+      pm.post = post_stab && pm.it == its;
+      pm.dual = on && pm.it >= 1;
+      pm.finalize = on && pm.it == its && its >= 1;
+      act = act && on;
+      solve = act && (pm.it < its || post_stab);
+    }
     if (pm.finalize && valid && lane == 0) finalize_body(d, i, dt);
     Acc s;
     acc_zero(s);
@@ -553,20 +580,23 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
         }
       }
     }
-    if (act && lane == 0) solve_body(d, i, xi4, qi, s, dt);
+    if (solve && lane == 0) solve_body(d, i, xi4, qi, s, dt);
   }
   if (pm.viol_slot >= 0) record_violation(d, pm.viol_slot, vmax, csum, ccnt);
 }
 
+// B: batched scenes (a separate instantiation, so the single-scene sweep's
+// register allocation does not carry the per-scene state).
+template <bool B>
 __device__ void ph_primal(const Dev& d, int c, PassMode pm, int gtid, int gsize) {
   float dt = d.prm->dt;
   switch (d.prm->group_size) {
-    case 1: primal_color<1>(d, c, pm, dt, gtid, gsize); break;
-    case 2: primal_color<2>(d, c, pm, dt, gtid, gsize); break;
-    case 4: primal_color<4>(d, c, pm, dt, gtid, gsize); break;
-    case 8: primal_color<8>(d, c, pm, dt, gtid, gsize); break;
-    case 16: primal_color<16>(d, c, pm, dt, gtid, gsize); break;
-    default: primal_color<32>(d, c, pm, dt, gtid, gsize); break;
+    case 1: primal_color<1, B>(d, c, pm, dt, gtid, gsize); break;
+    case 2: primal_color<2, B>(d, c, pm, dt, gtid, gsize); break;
+    case 4: primal_color<4, B>(d, c, pm, dt, gtid, gsize); break;
+    case 8: primal_color<8, B>(d, c, pm, dt, gtid, gsize); break;
+    case 16: primal_color<16, B>(d, c, pm, dt, gtid, gsize); break;
+    default: primal_color<32, B>(d, c, pm, dt, gtid, gsize); break;
   }
 }
 
@@ -577,7 +607,8 @@ __device__ __forceinline__ PassMode pass_mode(const DevParams& P, int it) {
   pm.post = P.post_stab && it == iters;
   pm.dual = it >= 1 && it <= iters;  // dual of iteration it-1
   pm.finalize = P.post_stab && it == iters && iters >= 1;
-  pm.viol_slot = (P.record_violation && pm.dual && it - 1 < 64) ? it - 1 : -1;
+  pm.viol_slot = (P.record_violation && pm.dual && it - 1 < 64 && !P.batched) ? it - 1 : -1;
+  pm.it = it;
   return pm;
 }
 
@@ -677,11 +708,13 @@ __device__ __forceinline__ void prelude_group(const Dev& d, int g, int fl, float
   }
 }
 
+template <bool B>
 __device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
   int ng = n_groups_live(d);
   for (int g = gtid; g < ng; g += gsize) {
     int fl = d.g_flags[g];
     if (fl & FL_NEW) continue;  // its prelude runs in ph_mlp_prelude
+    if (B && !group_on(d, g)) continue;  // batched: its scene sits this substep out
     prelude_group(d, g, fl, d.g_lam[g], d.g_pen[g]);
   }
 }
@@ -715,6 +748,7 @@ __device__ __noinline__ void ph_mlp_prelude(const Dev& d, int gtid, int gsize) {
         int k = r0 + row;
         const float* f = d.mlp_feat + (size_t)k * MLP_IN;
         int g = d.new_list[k];
+        if (!group_on(d, g)) continue;
         int fl = d.g_flags[g];
         float4 lam = d.g_lam[g], pen = d.g_pen[g];  // the zero start written by the emission
         float4 l2;
@@ -778,12 +812,18 @@ __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
 // Inertial target + warm start (kernels_6dof.py:122-187), plus the owner of
 // every contact group for the fused dual: its dynamic body with the lower
 // color (a static body never runs a primal, so it never owns).
+template <bool B>
 __device__ void ph_predict(const Dev& d, int gtid, int gsize) {
   const DevParams& P = *d.prm;
-  float dt = P.dt;
   for (int i = gtid; i < d.nb; i += gsize) {
+    float dt = P.dt;
     float4 x = d.x[i], q = d.q[i];
     float m = x.w;
+    if (B) {
+      float4 t = scene_entry(d, i);
+      if (!scene_on(d, t)) continue;  // the scene sits this substep out: state untouched
+      dt = t.x;
+    }
     d.x0[i] = x;
     d.q0[i] = q;
     M3 R = qmat(q);
@@ -1106,7 +1146,7 @@ __device__ void ph_bucket_place(const Dev& d) {
 // Two register budgets of the same kernel: 2 CTAs/SM (128 registers) or
 // 3 CTAs/SM (80 registers); the host picks one (params.blocks_per_sm).
 
-template <int MINB>
+template <int MINB, bool BATCHED>
 __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __grid_constant__ Dev d) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   int gsize = gridDim.x * blockDim.x;
@@ -1132,7 +1172,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
     d.ctr->n_marks = 1;
   }
   ph_gate(d, gtid, gsize);
-  ph_prelude(d, gtid, gsize);  // reads x/q = the initial pose; predict runs after
+  ph_prelude<BATCHED>(d, gtid, gsize);  // reads x/q = the initial pose; predict runs after
   ph_mlp_prelude(d, gtid, gsize);
   SYNC(PH_GATE_PRELUDE);
   if (recolor_needed(d)) {
@@ -1166,10 +1206,12 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
   } else if (gtid == 0) {
     d.ctr->recolored = 0;
   }
-  ph_predict(d, gtid, gsize);
+  ph_predict<BATCHED>(d, gtid, gsize);
   SYNC(PH_PREDICT);
   int iters = P.iterations;
-  int total = iters + (P.post_stab ? 1 : 0);
+  // batched scenes: one pass beyond the most iterations, where each scene
+  // runs its post-stab pass or its last dual + finalize
+  int total = iters + ((P.post_stab || P.batched) ? 1 : 0);
   int nc = *(volatile int*)&d.ctr->n_colors;
   // Pass `it` applies iteration it-1's dual update inside the color passes
   // (owner-first), so each iteration is nc barriers; without a
@@ -1177,11 +1219,11 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
   for (int it = 0; it < total; ++it) {
     PassMode pm = pass_mode(P, it);
     for (int c = 0; c < nc; ++c) {
-      ph_primal(d, c, pm, gtid, gsize);
+      ph_primal<BATCHED>(d, c, pm, gtid, gsize);
       SYNC(PH_PRIMAL);
     }
   }
-  if (!P.post_stab && iters >= 1) {
+  if (!P.post_stab && !P.batched && iters >= 1) {
     ph_dual(d, iters - 1, gtid, gsize);
     ph_finalize(d, gtid, gsize);
     SYNC(PH_DUAL);
@@ -1199,7 +1241,12 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
 // Split path: one launch per phase, same phase functions.
 // ---------------------------------------------------------------------------
 #define GS int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x
-__global__ void ks_gate_prelude(const __grid_constant__ Dev d) { GS; ph_gate(d, gtid, gsize); ph_prelude(d, gtid, gsize); }
+__global__ void ks_gate_prelude(const __grid_constant__ Dev d) {
+  GS;
+  ph_gate(d, gtid, gsize);
+  if (d.prm->batched) ph_prelude<true>(d, gtid, gsize);
+  else ph_prelude<false>(d, gtid, gsize);
+}
 __global__ void ks_mlp_prelude(const __grid_constant__ Dev d) { GS; ph_mlp_prelude(d, gtid, gsize); }
 __global__ void ks_color_reset(const __grid_constant__ Dev d) {
   GS;
@@ -1246,16 +1293,21 @@ __global__ void ks_bucket_place(const __grid_constant__ Dev d) {
   if (!d.ctr->recolored) return;
   ph_bucket_place(d);
 }
-__global__ void ks_predict(const __grid_constant__ Dev d) { GS; ph_predict(d, gtid, gsize); }
+__global__ void ks_predict(const __grid_constant__ Dev d) {
+  GS;
+  if (d.prm->batched) ph_predict<true>(d, gtid, gsize);
+  else ph_predict<false>(d, gtid, gsize);
+}
 __global__ void ks_primal(const __grid_constant__ Dev d, int it, int c) {
   GS;
   if (c >= d.ctr->n_colors) return;
-  ph_primal(d, c, pass_mode(*d.prm, it), gtid, gsize);
+  if (d.prm->batched) ph_primal<true>(d, c, pass_mode(*d.prm, it), gtid, gsize);
+  else ph_primal<false>(d, c, pass_mode(*d.prm, it), gtid, gsize);
 }
 __global__ void ks_tail(const __grid_constant__ Dev d) {
   GS;
   int iters = d.prm->iterations;
-  if (!d.prm->post_stab && iters >= 1) {
+  if (!d.prm->post_stab && !d.prm->batched && iters >= 1) {
     ph_dual(d, iters - 1, gtid, gsize);
     ph_finalize(d, gtid, gsize);
   }
@@ -1273,8 +1325,15 @@ int solve_occupancy(int block, int variant) {
   int n = 0;
   // sized with the learned warm start's shared weights, whether used or not
   size_t smem = sizeof(float) * AVBD_MLP_FLOATS;
-  if (variant >= 3) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<3>, block, smem);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<2>, block, smem);
+  int nb = 0;
+  if (variant >= 3) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<3, false>, block, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_solve_persistent<3, true>, block, smem);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_solve_persistent<2, false>, block, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_solve_persistent<2, true>, block, smem);
+  }
+  if (nb < n) n = nb;  // one grid size serves both instantiations
   return n;
 }
 
@@ -1285,7 +1344,9 @@ cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, 
   if (persistent) {
     void* args[] = {(void*)&d};
     g_kernel_launches += 1;
-    const void* fn = variant >= 3 ? (const void*)k_solve_persistent<3> : (const void*)k_solve_persistent<2>;
+    const bool b = d.n_scenes > 0;
+    const void* fn = variant >= 3 ? (b ? (const void*)k_solve_persistent<3, true> : (const void*)k_solve_persistent<3, false>)
+                                  : (b ? (const void*)k_solve_persistent<2, true> : (const void*)k_solve_persistent<2, false>);
     return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, mlp_smem, st);
   }
   ks_gate_prelude<<<grid, block, 0, st>>>(d);
@@ -1306,7 +1367,7 @@ cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, 
   ks_bucket_scan<<<1, block, 0, st>>>(d);
   ks_bucket_place<<<NCH, block, 0, st>>>(d);
   ks_predict<<<grid, block, 0, st>>>(d);
-  int total = P.iterations + (P.post_stabilize ? 1 : 0);
+  int total = P.iterations + ((P.post_stabilize || d.n_scenes > 0) ? 1 : 0);
   for (int it = 0; it < total; ++it)
     for (int c = 0; c < MAX_COLORS; ++c) ks_primal<<<grid, block, 0, st>>>(d, it, c);
   ks_tail<<<grid, block, 0, st>>>(d);

@@ -217,6 +217,11 @@ class Solver6DOF:
         self._debug_skip_arrive = False
         self._mlp = mlp_warm_start
         self._log_new = False
+        # batched scenes (avbd_b200.batch.SceneBatch): scene of each body and
+        # per scene (substeps per frame, iterations); empty for one scene
+        self._scene_of: list[int] = []
+        self._scene_tab: list[tuple[int, int]] = []
+        self._cur_scene = -1
 
         self._x, self._q, self._v, self._omega = [], [], [], []
         self._mass, self._half_extents, self._friction = [], [], []
@@ -266,6 +271,10 @@ class Solver6DOF:
         hx, hy, hz = (float(h) for h in half_extents)
         self._half_extents.append((hx, hy, hz))
         self._friction.append(max(0.0, float(friction)))
+        if self._scene_tab:
+            if self._cur_scene < 0:
+                raise RuntimeError("a batched solver needs a current scene (SceneBatch.add_scene) for add_box")
+            self._scene_of.append(self._cur_scene)
         self._dirty = True
         return RigidBody(index=idx, half_extents=(hx, hy, hz))
 
@@ -383,6 +392,7 @@ class Solver6DOF:
         # new-contact queue: allocated only when a warm-start model or the
         # training log can use it
         d.new_cap = max(1024, 8 * n) if self._self_collide and (self._mlp is not None or self._log_new) else 0
+        d.n_scenes = len(self._scene_tab)
         return d
 
     def _views(self):
@@ -509,6 +519,10 @@ class Solver6DOF:
                 dst[:k].copy_(src)
         if self._mlp is not None:
             self._arena.view("MLP_W", torch.float32, (self._mlp.n_floats,)).copy_(self._mlp.packed(dev))
+        if self._scene_tab:
+            if len(self._scene_of) != n:
+                raise RuntimeError("every body of a batched solver must belong to a scene")
+            self._arena.view("SCENE_OF", torch.int32, (n,)).copy_(torch.tensor(self._scene_of, dtype=torch.int32))
         L = _lib.load()
         ctx = C.c_void_p()
         _lib.check(L.avbd_create(C.byref(dims), C.c_void_p(self._arena.ptr()), self._arena.total, C.byref(ctx)),
@@ -554,13 +568,21 @@ class Solver6DOF:
         p.blocks_per_sm = int(self.blocks_per_sm)
         p.timing = int(self.timing)
         p.log_new_contacts = int(self._log_new)
+        if self._scene_tab:  # the device loops cover the largest scene settings
+            p.substeps = max(sc for sc, _ in self._scene_tab)
+            p.iterations = max(it for _, it in self._scene_tab)
         return p
 
     def _push_params(self):
         p = self._params()
-        key = bytes(p)
+        key = bytes(p) + repr(self._scene_tab).encode()
         if getattr(self, "_pushed", None) != key:
             _lib.check(_lib.load().avbd_set_params(self._ctx, C.byref(p), self._stream()), "set_params")
+            if self._scene_tab:  # per scene: (substep dt, iterations, substeps, 0)
+                tab = torch.tensor([(self.dt / sc, float(it), float(sc), 0.0) for sc, it in self._scene_tab],
+                                   dtype=torch.float32)
+                with torch.cuda.stream(self._cuda_stream):
+                    self._arena.view("SCENE_TAB", torch.float32, (len(self._scene_tab), 4)).copy_(tab)
             self._pushed = key
 
     def _current_graph_signature(self) -> tuple:

@@ -56,6 +56,12 @@ typedef struct AvbdDims {
   int mlp_floats;      /* learned warm-start weights: 0 or AVBD_MLP_FLOATS */
   int new_cap;         /* new contacts queued per substep for the learned
                           warm start / training log (0 = none) */
+  int n_scenes;        /* batched independent scenes (0 = one scene).  With
+                          n > 0 the arena's SCENE_OF gives each body's scene
+                          and SCENE_TAB per scene (substep dt, iterations,
+                          substeps per frame, 0) as float4; bodies of
+                          different scenes never collide.  AvbdParams then
+                          gives the maximum iterations and substeps. */
 } AvbdDims;
 
 /* Scalars of Solver6DOF.__init__ (solver_6dof.py:180-201). */

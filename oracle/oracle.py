@@ -169,6 +169,10 @@ class OracleSolver6DOF:
         self._rows: list[_Row] = []
         self._self_collide = False
         self._self_friction = 0.0
+        # coloring priorities: the reference's seeded draw over this solver's
+        # bodies, unless a checker sets them (a scene cut out of a batch keeps
+        # the batch's priorities)
+        self.priorities = None
         self._h = lib().orc_create(self.precision)
         self._dirty = True
         self.pair_cap = 0
@@ -259,7 +263,7 @@ class OracleSolver6DOF:
         iloc = np.stack([box_inertia_diag(m, *h) for m, h in zip(self._mass, self._he)]) if n else np.zeros((0, 3),
                                                                                                          np.float32)
         iloc = np.ascontiguousarray(iloc, np.float32)
-        prio = body_priorities(n)
+        prio = body_priorities(n) if self.priorities is None else np.ascontiguousarray(self.priorities, np.float32)
         rows = self._rows
         nr = len(rows)
         ia = lambda f: np.array([f(r) for r in rows], np.int32) if nr else np.zeros(0, np.int32)
