@@ -146,16 +146,34 @@ def c4_scene(sc: Scene, n_bodies: int, rng: np.random.Generator) -> None:
                 k += 1
 
 
-def c4_batch(n_scenes: int = 512, seed: int = 0, min_bodies: int = 16, max_bodies: int = 2048,
-             substep_choices=(2, 4, 8), iteration_choices=(5, 10, 20), **solver_kw) -> SceneBatch:
-    """The batched benchmark's scene set: body counts log-uniform in
-    [min_bodies, max_bodies], substeps and iterations drawn per scene."""
+def c4_specs(n_scenes: int = 512, seed: int = 0, min_bodies: int = 16, max_bodies: int = 2048,
+             substep_choices=(2, 4, 8), iteration_choices=(5, 10, 20)) -> list:
+    """Per scene (bodies, substeps, iterations, scene seed) of the batched
+    benchmark: body counts log-uniform in [min_bodies, max_bodies]."""
     rng = np.random.default_rng(seed)
-    kw = dict(friction_static_mult=1.25, coloring_mode="jones_plassmann")
+    out = []
+    for k in range(n_scenes):
+        n = int(round(math.exp(rng.uniform(math.log(min_bodies), math.log(max_bodies)))))
+        out.append((n, int(rng.choice(substep_choices)), int(rng.choice(iteration_choices)), seed * 100003 + k))
+    return out
+
+
+def c4_batch(specs, **solver_kw) -> SceneBatch:
+    """A SceneBatch holding the scenes of `specs` (see c4_specs)."""
+    kw = dict(friction_static_mult=1.25, coloring_mode="jones_plassmann", spacing=40.0)
     kw.update(solver_kw)
     batch = SceneBatch(**kw)
-    for _ in range(n_scenes):
-        n = int(round(math.exp(rng.uniform(math.log(min_bodies), math.log(max_bodies)))))
-        sc = batch.add_scene(substeps=int(rng.choice(substep_choices)), iterations=int(rng.choice(iteration_choices)))
-        c4_scene(sc, n, rng)
+    for n, sub, its, sseed in specs:
+        c4_scene(batch.add_scene(substeps=sub, iterations=its), n, np.random.default_rng(sseed))
     return batch
+
+
+def c4_single(spec, **solver_kw) -> Solver6DOF:
+    """One scene of `specs` as its own Solver6DOF (the one-at-a-time baseline)."""
+    n, sub, its, sseed = spec
+    kw = dict(friction_static_mult=1.25, coloring_mode="jones_plassmann")
+    kw.update(solver_kw)
+    s = Solver6DOF(dt=1.0 / 60.0, substeps=sub, iterations=its, **kw)
+    s.enable_self_collision(True, default_friction=0.0)
+    c4_scene(s, n, np.random.default_rng(sseed))
+    return s

@@ -374,6 +374,92 @@ def run_gpu(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_batched(args) -> None:
+    """Batched scenes: 512 independent scenes (bodies log-uniform in
+    [16, 2048], OBB heap distribution, per-scene friction, substeps in
+    {2, 4, 8}, iterations in {5, 10, 20}) stepped by one solver -- one
+    collision graph and one persistent solve launch per substep slot --
+    against launching the scenes one at a time (one Solver6DOF each, every
+    scene's frame enqueued back to back, one synchronisation per frame), on
+    the first `--seq-scenes` scenes for the ratio."""
+    import torch
+    from avbd_b200.autotune import autotune
+    from avbd_b200.batch import c4_batch, c4_single, c4_specs
+
+    specs = c4_specs(512, seed=0)
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+
+    def time_frames(step_all, sync, frames):
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        t0.record()
+        for _ in range(frames):
+            step_all()
+        sync()
+        t1.record()
+        torch.cuda.synchronize(dev)
+        return t0.elapsed_time(t1) / 1e3
+
+    def batched(spec_list, frames):
+        b = c4_batch(spec_list)
+        for _ in range(args.settle_batched):
+            b.solver._enqueue_step()
+        b.solver._after_frame()
+        tuned = autotune(b.solver) if not args.no_tune else None
+        for _ in range(args.warmup):
+            b.step()
+        st = b.solver._cuda_stream
+        k0 = b.stats()["kernels_launched"]
+        sec = time_frames(lambda: b.solver._enqueue_step(), lambda: st.synchronize(), frames)
+        b.solver._after_frame()
+        units = b.body_substeps_per_frame() * frames
+        return {"value": units / sec, "ms_per_frame": 1e3 * sec / frames,
+                "launches_per_frame": (b.stats()["kernels_launched"] - k0) / frames,
+                "bodies": len(b.solver._mass), "static_rows": len(b.solver._rows),
+                "launch_shape": tuned["best"] if tuned else None}
+
+    def one_at_a_time(spec_list, frames):
+        ss = [c4_single(sp) for sp in spec_list]
+        for s in ss:
+            for _ in range(args.settle_batched):
+                s._enqueue_step()
+            s._after_frame()
+            for _ in range(args.warmup):
+                s.step()
+
+        def step_all():
+            for s in ss:
+                s._enqueue_step()
+
+        def sync():
+            for s in ss:
+                s._cuda_stream.synchronize()
+
+        sec = time_frames(step_all, sync, frames)
+        for s in ss:
+            s._after_frame()
+        units = sum(sum(1 for m in s._mass if m > 0) * s.substeps for s in ss) * frames
+        return {"value": units / sec, "ms_per_frame": 1e3 * sec / frames}
+
+    full = batched(specs, args.steps)
+    sub = specs[: args.seq_scenes]
+    b_sub = batched(sub, args.steps)
+    seq = one_at_a_time(sub, max(3, args.steps // 3))
+    line = {"metric": "body-substeps/s, 512 batched scenes", "value": full["value"], "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": full["ms_per_frame"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": (f"512 scenes, bodies log-uniform [16, 2048] ({full['bodies']} bodies incl. 4 "
+                                    f"walls per scene, {full['static_rows']} static rows), OBB heaps, mu_s U[0.3,0.8], "
+                                    f"substeps {{2,4,8}}, iterations {{5,10,20}}, settled {args.settle_batched} "
+                                    "frames"),
+                       "launch_shape": full["launch_shape"], "launches_per_frame": full["launches_per_frame"]},
+            "one_at_a_time": {"scenes": len(sub), "batched": b_sub["value"], "one_at_a_time": seq["value"],
+                              "speedup": b_sub["value"] / seq["value"],
+                              "ms_per_frame": {"batched": b_sub["ms_per_frame"],
+                                               "one_at_a_time": seq["ms_per_frame"]}}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,11 +474,16 @@ def main():
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="solve CTAs per SM (0 = autotuned)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start evaluation")
+    ap.add_argument("--batched", action="store_true", help="512 batched scenes vs one scene at a time")
+    ap.add_argument("--seq-scenes", type=int, default=64, help="scenes in the one-at-a-time comparison")
+    ap.add_argument("--settle-batched", type=int, default=60)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.batched:
+        run_batched(args)
     else:
         run_gpu(args)
 
