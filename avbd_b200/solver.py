@@ -95,12 +95,96 @@ class _Row:  # solver_6dof.py:113-129
     partner: int = -1
 
 
+# Corner order of add_floor_contact_box (solver_6dof.py:474-520): x outer, z inner.
+_CORNER_SIGNS = np.array([(sx, sy, sz) for sx in (-1.0, 1.0) for sy in (-1.0, 1.0) for sz in (-1.0, 1.0)])
+
+
+class _RowTable:
+    """The reference's constraint-row list (row numbering of the c_* arrays,
+    solver_6dof.py:1067-1129), stored compactly: explicit rows (pins) plus
+    one record per add_floor_contact_box call, whose 8 corners x (1 or 3)
+    rows are materialised only when a row is looked up.  A 100k-box pile has
+    2.4 M floor rows; they exist here as 100 k block records, and the
+    static groups are built from them with array operations."""
+
+    def __init__(self):
+        self._starts: list[int] = []  # first row of each segment
+        self._segs: list = []  # list[_Row] (explicit rows) or a floor-block tuple
+        self._n = 0
+
+    def __len__(self) -> int:
+        return self._n
+
+    def append(self, row: _Row) -> None:
+        if not self._segs or not isinstance(self._segs[-1], list):
+            self._starts.append(self._n)
+            self._segs.append([])
+        self._segs[-1].append(row)
+        self._n += 1
+
+    def add_floor_block(self, body: int, he: tuple, floor_y: float, mu: float, mus: float,
+                        stiffness: float) -> int:
+        start = self._n
+        per = 3 if mu > 0.0 else 1
+        self._starts.append(start)
+        self._segs.append((body, he, floor_y, mu, mus, stiffness, start, per))
+        self._n += 8 * per
+        return start
+
+    @staticmethod
+    def _block_row(blk, k: int) -> _Row:
+        body, he, floor_y, mu, mus, stiff, start, per = blk
+        c, s = divmod(k, per)
+        off = tuple(float(v) for v in _CORNER_SIGNS[c] * np.asarray(he))
+        n = start + c * per
+        if s == 0:
+            return _Row(FLOOR_CONTACT_6DOF, body, world_anchor=(0.0, float(floor_y), 0.0), off_a=off,
+                        stiffness=stiff, fmin=-_INF, fmax=0.0)
+        t = n + 1
+        return _Row(CONTACT_TANGENT_6DOF, body, world_anchor=(1.0, 0.0, 0.0) if s == 1 else (0.0, 0.0, 1.0),
+                    off_a=off, stiffness=stiff, sibling=n, friction=mu, friction_static=mus,
+                    partner=t + 1 if s == 1 else t)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[k] for k in range(*i.indices(self._n))]
+        if i < 0:
+            i += self._n
+        if not 0 <= i < self._n:
+            raise IndexError(i)
+        j = int(np.searchsorted(self._starts, i, side="right")) - 1
+        seg = self._segs[j]
+        k = i - self._starts[j]
+        return seg[k] if isinstance(seg, list) else self._block_row(seg, k)
+
+    def __iter__(self):
+        for j, seg in enumerate(self._segs):
+            if isinstance(seg, list):
+                yield from seg
+            else:
+                for k in range(8 * seg[7]):
+                    yield self._block_row(seg, k)
+
+    def floor_blocks(self) -> list:
+        return [seg for seg in self._segs if not isinstance(seg, list)]
+
+
 def box_inertia_local(mass: float, hx: float, hy: float, hz: float) -> np.ndarray:
     """Solid-box body inertia (solver_6dof.py:132-142); zero for static bodies."""
     if mass <= 0.0:
         return np.zeros((3, 3), dtype=np.float32)
     return np.diag([mass / 3.0 * (hy * hy + hz * hz), mass / 3.0 * (hx * hx + hz * hz),
                     mass / 3.0 * (hx * hx + hy * hy)]).astype(np.float32)
+
+
+def _box_inertia_diag_batch(mass: np.ndarray, he: np.ndarray) -> np.ndarray:
+    """box_inertia_local's diagonal for arrays of bodies (same float64
+    arithmetic, then float32)."""
+    hx, hy, hz = he[:, 0], he[:, 1], he[:, 2]
+    d = np.stack([mass / 3.0 * (hy * hy + hz * hz), mass / 3.0 * (hx * hx + hz * hz),
+                  mass / 3.0 * (hx * hx + hy * hy)], 1)
+    d[mass <= 0.0] = 0.0
+    return d.astype(np.float32)
 
 
 def box_inv_inertia_local(mass: float, hx: float, hy: float, hz: float) -> np.ndarray:
@@ -225,8 +309,10 @@ class Solver6DOF:
 
         self._x, self._q, self._v, self._omega = [], [], [], []
         self._mass, self._half_extents, self._friction = [], [], []
-        self._rows: list[_Row] = []
-        self._groups: list[tuple] = []  # (kind, body, row0, three, off, extra3, mu, mus, stiffness, fracture)
+        self._rows = _RowTable()
+        # explicit static groups (pins): (kind, body, row0, three, off, extra3, mu, mus, stiffness, fracture);
+        # floor-contact groups live in the row table's floor blocks (8 each)
+        self._groups: list[tuple] = []
         self._dirty = True
         self._self_collide = False
         self._self_friction = 0.0
@@ -281,28 +367,11 @@ class Solver6DOF:
     def add_floor_contact_box(self, body: RigidBody, floor_y: float = 0.0, friction=None,
                               stiffness: float = _INF) -> list[int]:
         mu = float(friction) if friction is not None else self._friction[body.index]
-        hx, hy, hz = body.half_extents
-        out = []
-        for sx in (-1.0, 1.0):
-            for sy in (-1.0, 1.0):
-                for sz in (-1.0, 1.0):
-                    off = (sx * hx, sy * hy, sz * hz)
-                    n = len(self._rows)
-                    self._rows.append(_Row(FLOOR_CONTACT_6DOF, body.index, world_anchor=(0.0, float(floor_y), 0.0),
-                                           off_a=off, stiffness=stiffness, fmin=-_INF, fmax=0.0))
-                    out.append(n)
-                    mus = 0.0
-                    if mu > 0.0:
-                        mus = mu * self.friction_static_mult
-                        t = len(self._rows)
-                        self._rows.append(_Row(CONTACT_TANGENT_6DOF, body.index, world_anchor=(1.0, 0.0, 0.0),
-                                               off_a=off, stiffness=stiffness, sibling=n, friction=mu,
-                                               friction_static=mus, partner=t + 1))
-                        self._rows.append(_Row(CONTACT_TANGENT_6DOF, body.index, world_anchor=(0.0, 0.0, 1.0),
-                                               off_a=off, stiffness=stiffness, sibling=n, friction=mu,
-                                               friction_static=mus, partner=t))
-                    self._groups.append((KIND_FLOOR, body.index, n, mu > 0.0, off, (0.0, float(floor_y), 0.0),
-                                         mu, mus, float(stiffness), _INF))
+        mus = mu * self.friction_static_mult if mu > 0.0 else 0.0
+        start = self._rows.add_floor_block(body.index, tuple(float(h) for h in body.half_extents), float(floor_y),
+                                           mu, mus, float(stiffness))
+        per = 3 if mu > 0.0 else 1
+        out = [start + c * per for c in range(8)]
         self._dirty = True
         return out
 
@@ -382,7 +451,7 @@ class Solver6DOF:
             pc, dr, hc = 0, 0, 1024
         d = _lib.AvbdDims()
         d.n_bodies = n
-        d.n_static_groups = len(self._groups)
+        d.n_static_groups = self._n_static_groups
         d.n_static_rows = len(self._rows)
         d.pair_cap = pc
         d.dyn_row_cap = dr
@@ -428,42 +497,77 @@ class Solver6DOF:
         self._h_s0 = A.view("H_S0", torch.float32, (h, 4))
         self._h_s1 = A.view("H_S1", torch.float32, (h, 4))
 
+    @property
+    def _n_static_groups(self) -> int:
+        return 8 * len(self._rows.floor_blocks()) + len(self._groups)
+
     def _static_group_arrays(self):
-        """Static groups sorted by body (stable), so each body's groups are one
-        contiguous range; returns numpy arrays and the static row -> (group,
-        slot) map."""
+        """Static groups sorted by body (stable: by first row within a body),
+        so each body's groups are one contiguous range; returns numpy arrays
+        and the static row -> (group, slot) map.  Floor corners are expanded
+        from their block records with array operations."""
         n = len(self._x)
-        gs = self._groups
-        order = sorted(range(len(gs)), key=lambda k: gs[k][1])
-        ng = len(gs)
-        body = np.full((max(ng, 1), 2), -1, np.int32)
-        meta = np.zeros(max(ng, 1), np.int32)
-        row0 = np.zeros(max(ng, 1), np.int32)
-        offa = np.zeros((max(ng, 1), 4), np.float32)
-        gn = np.zeros((max(ng, 1), 4), np.float32)
-        mat = np.zeros((max(ng, 1), 4), np.float32)
-        flags = np.zeros(max(ng, 1), np.int32)
-        row_map = np.zeros((len(self._rows), 2), np.int64)
-        for new, k in enumerate(order):
-            kind, b, r0, three, off, extra, mu, mus, stiff, frac = gs[k]
-            body[new] = (b, -1)
+        fb = self._rows.floor_blocks()
+        nf = 8 * len(fb)
+        ng = nf + len(self._groups)
+        G = max(ng, 1)
+        body = np.full((G, 2), -1, np.int32)
+        meta = np.zeros(G, np.int32)
+        row0 = np.zeros(G, np.int64)
+        offa = np.zeros((G, 4), np.float32)
+        gn = np.zeros((G, 4), np.float32)
+        mat = np.zeros((G, 4), np.float32)
+        three = np.zeros(G, bool)
+        if fb:
+            bb = np.array([f[0] for f in fb], np.int64)
+            he = np.array([f[1] for f in fb], np.float64)
+            fy = np.array([f[2] for f in fb], np.float32)
+            mu = np.array([f[3] for f in fb], np.float32)
+            mus = np.array([f[4] for f in fb], np.float32)
+            st = np.array([f[5] for f in fb], np.float32)
+            r0 = np.array([f[6] for f in fb], np.int64)
+            per = np.array([f[7] for f in fb], np.int64)
+            body[:nf, 0] = np.repeat(bb, 8)
+            offa[:nf, :3] = (he[:, None, :] * _CORNER_SIGNS[None, :, :]).reshape(-1, 3).astype(np.float32)
+            offa[:nf, 3] = np.repeat(fy, 8)
+            row0[:nf] = (r0[:, None] + np.arange(8)[None, :] * per[:, None]).reshape(-1)
+            three[:nf] = np.repeat(per == 3, 8)
+            hard = np.repeat(~(st < _INF), 8)
+            meta[:nf] = KIND_FLOOR | np.where(three[:nf], 4, 0) | np.where(hard, 8, 0)
+            mat[:nf] = np.repeat(np.stack([mu, mus, st, np.full_like(st, _INF)], 1), 8, axis=0)
+        for j, (kind, b, r0_, th, off, extra, mu_, mus_, stiff, frac) in enumerate(self._groups):
+            k = nf + j
+            body[k, 0] = b
             hard = not (stiff < _INF)
-            meta[new] = kind | (4 if three else 0) | (8 if hard else 0)
-            row0[new] = r0
-            offa[new, :3] = off
+            meta[k] = kind | (4 if th else 0) | (8 if hard else 0)
+            row0[k] = r0_
+            three[k] = th
+            offa[k, :3] = off
             if kind == KIND_FLOOR:
-                offa[new, 3] = extra[1]
+                offa[k, 3] = extra[1]
             else:
-                gn[new, :3] = extra
-            mat[new] = (mu, mus, stiff, frac)
-            nr = 3 if three else 1
-            flags[new] = 7 if three else 1
-            for s in range(nr):
-                row_map[r0 + s] = (new, s)
-        counts = np.bincount(np.array([gs[k][1] for k in order], np.int64), minlength=n) if ng else np.zeros(n, np.int64)
+                gn[k, :3] = extra
+            mat[k] = (mu_, mus_, stiff, frac)
+        order = np.lexsort((row0[:ng], body[:ng, 0])) if ng else np.zeros(0, np.int64)
+        out = dict(body=body[order] if ng else body, meta=meta[order] if ng else meta,
+                   row0=(row0[order] if ng else row0).astype(np.int32), offa=offa[order] if ng else offa,
+                   n=gn[order] if ng else gn, mat=mat[order] if ng else mat)
+        th = three[order] if ng else three
+        out["flags"] = np.where(th, 7, 1).astype(np.int32)
+        row_map = np.zeros((len(self._rows), 2), np.int64)
+        if ng:
+            g_idx = np.arange(ng, dtype=np.int64)
+            r0s = out["row0"][:ng].astype(np.int64)
+            row_map[r0s, 0] = g_idx
+            row_map[r0s, 1] = 0
+            t = th[:ng]
+            for s_ in (1, 2):
+                row_map[r0s[t] + s_, 0] = g_idx[t]
+                row_map[r0s[t] + s_, 1] = s_
+        counts = np.bincount(body[:ng, 0].astype(np.int64), minlength=n) if ng else np.zeros(n, np.int64)
         sg_start = np.zeros(n + 1, np.int32)
         sg_start[1:] = np.cumsum(counts[:n])
-        return dict(body=body, meta=meta, row0=row0, offa=offa, n=gn, mat=mat, flags=flags), sg_start, row_map
+        return out, sg_start, row_map
 
     @_on_stream
     def _flush(self) -> None:
@@ -496,13 +600,13 @@ class Solver6DOF:
             he4[:, 3] = np.array(self._friction, np.float32)
             self._he4.copy_(torch.from_numpy(he4))
             il = np.zeros((n, 4), np.float32)
-            for i, (mm, h) in enumerate(zip(self._mass, self._half_extents)):
-                il[i, :3] = np.diag(box_inertia_local(mm, *h))
+            il[:, :3] = _box_inertia_diag_batch(np.asarray(self._mass, np.float64),
+                                                np.asarray(self._half_extents, np.float64))
             self._iloc4.copy_(torch.from_numpy(il))
             prio = np.random.default_rng(seed=0xA5BD).uniform(0.0, 1.0, size=n).astype(np.float32)
             self._prio.copy_(torch.from_numpy(prio))
         sg, sg_start, self._row_map = self._static_group_arrays()
-        ng = len(self._groups)
+        ng = self._n_static_groups
         if ng:
             self._g_body[:ng].copy_(torch.from_numpy(sg["body"][:ng]))
             self._g_meta[:ng].copy_(torch.from_numpy(sg["meta"][:ng]))
@@ -850,7 +954,7 @@ class Solver6DOF:
         if self._arena is None:
             act[: len(self._rows)] = 1
             return lam, pen, ac0, act, was, typ
-        ng = len(self._groups) + int(self._stats.n_dyn_groups)
+        ng = self._n_static_groups + int(self._stats.n_dyn_groups)
         ng = min(ng, self._g_meta.shape[0])
         meta = self._g_meta[:ng].cpu().numpy()
         row0 = self._g_row0[:ng].cpu().numpy()
@@ -986,18 +1090,24 @@ class Solver6DOF:
         ns = len(self._rows)
         if ns:
             rm = self._row_map
-            ng = len(self._groups)
+            ng = self._n_static_groups
             lam = self._g_lam[:ng].cpu().numpy()
             pen = self._g_pen[:ng].cpu().numpy()
             fl = self._g_flags[:ng].cpu().numpy()
             meta = self._g_meta[:ng].cpu().numpy()
-            for r in range(ns):
-                g, s = rm[r]
-                lam[g, s] = sd["row_lam"][r]
-                pen[g, s] = sd["row_pen"][r]
-                fl[g] = (fl[g] & ~(1 << s)) | (int(sd["row_active"][r]) << s)
-                if s == 0 and (meta[g] & 3) != KIND_PIN:
-                    fl[g] = (fl[g] & ~8) | (int(sd["row_was"][r]) << 3)
+            g_of, s_of = rm[:ns, 0], rm[:ns, 1]
+            lam[g_of, s_of] = np.asarray(sd["row_lam"], np.float32)[:ns]
+            pen[g_of, s_of] = np.asarray(sd["row_pen"], np.float32)[:ns]
+            act = np.asarray(sd["row_active"], np.int32)[:ns]
+            was = np.asarray(sd["row_was"], np.int32)[:ns]
+            for s in range(3):  # one row per group in each pass
+                m = s_of == s
+                g = g_of[m]
+                fl[g] = (fl[g] & ~(1 << s)) | (act[m] << s)
+                if s == 0:
+                    nonpin = (meta[g] & 3) != KIND_PIN
+                    g2 = g[nonpin]
+                    fl[g2] = (fl[g2] & ~8) | (was[m][nonpin] << 3)
             self._g_lam[:ng] = torch.from_numpy(lam).to(dev)
             self._g_pen[:ng] = torch.from_numpy(pen).to(dev)
             self._g_flags[:ng] = torch.from_numpy(fl).to(dev)
@@ -1036,7 +1146,7 @@ class Solver6DOF:
     @_on_stream
     def contacts(self) -> np.ndarray:
         """(ref body, inc body, ordinal) of every emitted dynamic contact, row order."""
-        ns = len(self._groups)
+        ns = self._n_static_groups
         nd = int(self._stats.n_dyn_groups)
         b = self._g_body[ns:ns + nd].cpu().numpy()
         meta = self._g_meta[ns:ns + nd].cpu().numpy()

@@ -241,7 +241,10 @@ def run_gpu(args) -> None:
         s.primal_group_size = args.group_size
     if args.blocks_per_sm:
         s.blocks_per_sm = args.blocks_per_sm
+    t_build = time.perf_counter()
     scenes.pile(s, **size)
+    s._flush()  # host scene build + arena upload, timed for the report
+    t_build = time.perf_counter() - t_build
     nb = dyn_bodies(s)
     for _ in range(args.settle):
         s._enqueue_step()
@@ -340,7 +343,7 @@ def run_gpu(args) -> None:
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": (f"pile {size['nx']}x{size['nz']}x{size['ny']} ({nb} OBBs, he U[0.2,0.4], "
-                                f"{sum(1 for r in s._rows if r.type == 2) // 3} corner pins fracture 5e4), dt 1/60, "
+                                f"{sum(1 for g in s._groups if g[0] == 1)} corner pins fracture 5e4), dt 1/60, "
                                 "4 substeps, 10 iterations + post-stab, JP coloring; settled "
                                 f"{args.settle} frames before warm-up"),
                    "global_batch": nb * world, "seq_len": None, "parallelism": f"replicas x{world}",
@@ -348,7 +351,8 @@ def run_gpu(args) -> None:
                    "live": {"dyn_rows": r2, "static_rows": r1, "pairs": int(st["n_pairs"]),
                             "contacts": int(st["n_dyn_groups"]), "colors": int(st["n_colors"])},
                    "launch_shape": {"group_size": s.primal_group_size, "blocks_per_sm": s.blocks_per_sm,
-                                    "autotuned": tuned is not None}},
+                                    "autotuned": tuned is not None},
+                   "scene_build_s": round(t_build, 2)},
         "roofline": {"bound": "hbm", "kernel": "k_solve_persistent", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": ab["solve"], "launch_ms": solve_ms,

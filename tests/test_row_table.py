@@ -1,0 +1,51 @@
+"""The compact row table behind Solver6DOF._rows: floor-contact blocks must
+materialise exactly the rows the reference's add_floor_contact_box appends
+(solver_6dof.py:474-520), in the same numbering, interleaved with explicit
+rows (pins) in call order."""
+
+import math
+
+import numpy as np
+
+from avbd_b200.solver import CONTACT_TANGENT_6DOF, FLOOR_CONTACT_6DOF, PIN_6DOF, _Row, _RowTable
+
+INF = math.inf
+
+
+def _expected_floor(rows, body, he, floor_y, mu, mus, stiff):
+    for sx in (-1.0, 1.0):
+        for sy in (-1.0, 1.0):
+            for sz in (-1.0, 1.0):
+                off = (sx * he[0], sy * he[1], sz * he[2])
+                n = len(rows)
+                rows.append(_Row(FLOOR_CONTACT_6DOF, body, world_anchor=(0.0, floor_y, 0.0), off_a=off,
+                                 stiffness=stiff, fmin=-INF, fmax=0.0))
+                if mu > 0.0:
+                    t = len(rows)
+                    rows.append(_Row(CONTACT_TANGENT_6DOF, body, world_anchor=(1.0, 0.0, 0.0), off_a=off,
+                                     stiffness=stiff, sibling=n, friction=mu, friction_static=mus, partner=t + 1))
+                    rows.append(_Row(CONTACT_TANGENT_6DOF, body, world_anchor=(0.0, 0.0, 1.0), off_a=off,
+                                     stiffness=stiff, sibling=n, friction=mu, friction_static=mus, partner=t))
+
+
+def test_row_table_matches_explicit_rows():
+    tab, ref = _RowTable(), []
+    rng = np.random.default_rng(0)
+    for k in range(40):
+        if k % 7 == 3:  # a pin: three explicit rows
+            for axis in range(3):
+                r = _Row(PIN_6DOF, k, body_b=axis, world_anchor=(1.0, 2.0, 3.0), off_a=(0.1, 0.2, 0.3))
+                tab.append(r)
+                ref.append(r)
+            continue
+        he = tuple(float(v) for v in rng.uniform(0.1, 0.5, 3))
+        mu = 0.0 if k % 5 == 0 else 0.4
+        start = tab.add_floor_block(k, he, 0.25 * (k % 3), mu, 1.25 * mu, INF if k % 4 else 1e7)
+        assert start == len(ref)
+        _expected_floor(ref, k, he, 0.25 * (k % 3), mu, 1.25 * mu, INF if k % 4 else 1e7)
+    assert len(tab) == len(ref)
+    assert list(tab) == ref
+    for i in rng.integers(0, len(ref), 50):
+        assert tab[int(i)] == ref[int(i)]
+    assert tab[-1] == ref[-1] and tab[3:9] == ref[3:9]
+    assert len(tab.floor_blocks()) == sum(1 for k in range(40) if k % 7 != 3)
