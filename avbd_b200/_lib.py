@@ -32,7 +32,8 @@ class AvbdParams(C.Structure):
                 ("recolor_every_substep", C.c_int), ("self_collide", C.c_int), ("self_friction", C.c_float),
                 ("group_size", C.c_int), ("use_graph", C.c_int), ("persistent", C.c_int),
                 ("record_violation", C.c_int), ("mlp_warm_start", C.c_int), ("debug_skip_arrive", C.c_int),
-                ("blocks_per_sm", C.c_int), ("timing", C.c_int), ("log_new_contacts", C.c_int)]
+                ("blocks_per_sm", C.c_int), ("timing", C.c_int), ("log_new_contacts", C.c_int),
+                ("flag_sweep", C.c_int)]
 
 
 class AvbdStats(C.Structure):

@@ -1,12 +1,15 @@
 """Launch-shape autotuner for the substep solve.
 
-Two knobs decide how the persistent solve kernel maps onto the 148 SMs:
+Three knobs decide how the persistent solve kernel maps onto the 148 SMs:
 
 * lanes per body in the primal sweep -- the reference's `primal_group_size`
   (src/avbd3d/solver_6dof.py:627-637; 1..32 lanes gather one body's
   constraint groups and reduce its 6x6 system by shuffles);
 * CTAs per SM of the cooperative grid (2 or 3; each count has its own
-  register budget, 128 or 80 registers per thread).
+  register budget, 128 or 80 registers per thread);
+* how the color passes are ordered: a grid barrier per color, or per-body
+  completion flags (each body waits only for its neighbours, so passes of
+  small colors overlap).
 
 The best pair depends on the scene: bodies per color, groups per body and
 whether the group records fit in L2.  `autotune` times every candidate on the
@@ -40,25 +43,29 @@ def _time_frames(solver, frames: int, warm: int) -> float:
     return ms / frames
 
 
-def autotune(solver, group_sizes=(4, 8, 16, 32), blocks_per_sm=(2, 3), frames: int = 2, warm: int = 1,
-             apply: bool = True) -> dict:
-    """Times each (group size, CTAs per SM) pair for `frames` frames and
-    returns {"best": {...}, "table": [...]}; sets the best pair on the solver
-    when `apply`.  The scene state is restored afterwards."""
+def autotune(solver, group_sizes=(4, 8, 16), blocks_per_sm=(2, 3), flag_sweep=(False, True), frames: int = 2,
+             warm: int = 1, apply: bool = True) -> dict:
+    """Times each (group size, CTAs per SM, sweep ordering) candidate for
+    `frames` frames and returns {"best": {...}, "table": [...]}; sets the
+    best candidate on the solver when `apply`.  The scene state is restored
+    afterwards."""
     solver._flush()
     sd = solver.state_dict()
-    g0, b0 = solver.primal_group_size, solver.blocks_per_sm
+    g0, b0, f0 = solver.primal_group_size, solver.blocks_per_sm, solver.flag_sweep
     table = []
-    for g, b in itertools.product(group_sizes, blocks_per_sm):
+    for g, b, f in itertools.product(group_sizes, blocks_per_sm, flag_sweep):
         solver.load_state_dict(sd)
         solver.primal_group_size = g
         solver.blocks_per_sm = b
-        table.append({"group_size": g, "blocks_per_sm": b, "ms_per_frame": _time_frames(solver, frames, warm)})
+        solver.flag_sweep = f
+        table.append({"group_size": g, "blocks_per_sm": b, "flag_sweep": f,
+                      "ms_per_frame": _time_frames(solver, frames, warm)})
     best = min(table, key=lambda r: r["ms_per_frame"])
     solver.load_state_dict(sd)
     if apply:
         solver.primal_group_size = best["group_size"]
         solver.blocks_per_sm = best["blocks_per_sm"]
+        solver.flag_sweep = best["flag_sweep"]
     else:
-        solver.primal_group_size, solver.blocks_per_sm = g0, b0
+        solver.primal_group_size, solver.blocks_per_sm, solver.flag_sweep = g0, b0, f0
     return {"best": best, "table": table}

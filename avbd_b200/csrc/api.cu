@@ -43,7 +43,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(H_S0, 16, H) X(H_S1, 16, H) X(SCAN_PART, 4, SP) X(SORT_HIST, 4, SH) X(C_USED, 4, N) X(C_LOST, 4, N)        \
   X(C_HIST, 4, 64 * 64) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
   X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
-  X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS)
+  X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS) X(DONE, 4, N)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,
@@ -204,6 +204,7 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.n_scenes = dims->n_scenes;
   d.scene_of = dims->n_scenes > 0 ? PTR(const int*, SCENE_OF) : nullptr;
   d.scene_tab = dims->n_scenes > 0 ? PTR(const float4*, SCENE_TAB) : nullptr;
+  d.done = PTR(int*, DONE);
   d.ctr = PTR(DevCounters*, COUNTERS);
 #undef PTR
   int occ = solve_occupancy(256, 2);
@@ -260,6 +261,7 @@ static void fill_devparams(AvbdCtx* c, float dt_sub) {
   q.mlp_on = P.mlp_warm_start && c->dims.mlp_floats > 0 && c->dims.new_cap > 0;
   q.log_new = P.log_new_contacts && c->dims.new_cap > 0;
   q.batched = c->dims.n_scenes > 0;
+  q.flag_sweep = P.flag_sweep;
   q.barrier_timeout_ns = P.debug_skip_arrive ? 200000000ull : 2000000000ull;
   q.timing = P.timing;
 }

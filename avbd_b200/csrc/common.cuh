@@ -144,7 +144,8 @@ struct DevParams {
   int timing;   // record phase timestamps in the counters
   int log_new;  // queue every new contact's features (training-data log)
   int batched;  // bodies belong to scenes with their own dt / iterations / substeps
-  int pad[5];
+  int flag_sweep;  // color passes ordered by per-body completion flags instead of grid barriers
+  int pad[4];
 };
 
 // Phase ids of the persistent kernel's timestamps.
@@ -203,6 +204,8 @@ struct Dev {
   int n_scenes;
   const int* scene_of;       // scene of each body
   const float4* scene_tab;   // per scene: (substep dt, iterations, substeps per frame, 0)
+  // flag-ordered sweep: passes each body has completed in this substep
+  int* done;
   // counters
   DevCounters* ctr;
 };

@@ -33,6 +33,49 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 
+// ---------------------------------------------------------------------------
+// Flag-ordered sweep primitives.  done[i] counts the color passes body i has
+// finished in this substep.  A finished body publishes with a release store
+// after its writes are fenced; a waiter polls with acquire loads, bounded by
+// prm->barrier_timeout_ns (then ERR_BARRIER_TIMEOUT is set and every wait of
+// the launch returns at once, so the kernel ends).
+// ---------------------------------------------------------------------------
+template <bool F, class T>
+__device__ __forceinline__ T ldm(const T* p) {
+  if constexpr (F) return __ldcg(p);  // written by another SM this substep: read through L2
+  else return *p;
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __noinline__ void wait_done_slow(const Dev& d, int o, int need) {
+  unsigned long long t0 = gtimer();
+  unsigned long long budget = d.prm->barrier_timeout_ns;
+  for (unsigned spins = 1;; ++spins) {
+    if (ld_acquire(d.done + o) >= need) return;
+    if ((spins & 31u) == 0u) {
+      if (*(volatile int*)&d.ctr->err & ERR_BARRIER_TIMEOUT) return;
+      if (gtimer() - t0 > budget) {
+        atomicOr(&d.ctr->err, ERR_BARRIER_TIMEOUT);
+        return;
+      }
+    }
+    __nanosleep(64);
+  }
+}
+
+__device__ __forceinline__ void wait_done(const Dev& d, int o, int need) {
+  if (ld_acquire(d.done + o) < need) wait_done_slow(d, o, need);
+}
+
 __device__ bool grid_barrier(const Dev& d, int idx) {
   __shared__ int ok;
   __syncthreads();
@@ -253,14 +296,33 @@ __device__ __forceinline__ void learned_check(const Dev& d, int kind, bool hard,
 // owner's color runs before the other body's.  Returns the violation of the
 // updated rows (0 when no dual ran); a box-box group's violation is also
 // added to csum / ccnt (the contact-row statistics of record_violation).
+//
+// F (flag-ordered sweep): before a box-box group's state and the other
+// body's pose are read, wait until the other body has finished the pass this
+// one needs -- pass it+1 when it owns the group (lower color, already updated
+// in this pass), pass it otherwise -- and read everything another SM may
+// have written in this substep through L2 (__ldcg), never through L1.
+template <bool F>
 __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3 xi, float4 qi, bool post, bool dual,
-                                                  Acc& s, float& csum, int& ccnt) {
+                                                  Acc& s, float& csum, int& ccnt, int it = 0, int ci = 0) {
   int meta = d.g_meta[g];
-  int fl = d.g_flags[g];
+  int fl = ldm<F>(d.g_flags + g);
   int kind = meta_kind(meta);
   bool three = (meta & 4) != 0, hard = (meta & 8) != 0;
   int nr = three ? 3 : 1;
-  float4 lam = d.g_lam[g], pen = d.g_pen[g], ac0 = d.g_ac0[g], mat = d.g_mat[g];
+  if (F && kind == KIND_BOX) {
+    int2 bd = d.g_body[g];
+    int o = bd.x == i ? bd.y : bd.x;
+    // A neighbour of the same color (a coloring that kept a conflict) runs
+    // concurrently, as in the barrier sweep; waiting there could deadlock.
+    if (d.color[o] != ci) {
+      bool own_b = (fl & FL_OWNB) != 0;  // set before the passes; stable during them
+      bool i_owns = own_b == (bd.y == i);
+      wait_done(d, o, i_owns ? it : it + 1);
+      fl = ldm<F>(d.g_flags + g);  // after the owner's dual update of this pass
+    }
+  }
+  float4 lam = ldm<F>(d.g_lam + g), pen = ldm<F>(d.g_pen + g), ac0 = d.g_ac0[g], mat = d.g_mat[g];
   float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z}, ac[3] = {ac0.x, ac0.y, ac0.z};
   float C[3] = {0.0f, 0.0f, 0.0f};
   V3 rs, dirs[3], dd;
@@ -284,7 +346,7 @@ __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3
     bool side_a = bd.x == i;
     own = ((fl & FL_OWNB) != 0) == !side_a;
     int o = side_a ? bd.y : bd.x;
-    float4 xo4 = d.x[o], qo = d.q[o];
+    float4 xo4 = ldm<F>(d.x + o), qo = ldm<F>(d.q + o);
     float4 oa = d.g_offa[g], ob = d.g_offb[g];
     V3 n = xyz(d.g_n[g]);
     if (side_a) {
@@ -464,16 +526,16 @@ __device__ __forceinline__ bool group_on(const Dev& d, int g) {
 }
 
 // BDF1 velocities + caps of one body (kernels_6dof.py:1871-1901).
-__device__ __forceinline__ void finalize_body(const Dev& d, int i, float dt) {
+// x, q: the body's current pose.
+__device__ __forceinline__ void finalize_body(const Dev& d, int i, float dt, float4 x, float4 q) {
   const DevParams& P = *d.prm;
   float4 v = d.v[i], w = d.w[i];
   d.pv[i] = v;
   d.pw[i] = w;
-  float4 x = d.x[i];
   if (x.w > 0.0f) {
     float4 x0 = d.x0[i];
     V3 nv = V3{x.x - x0.x, x.y - x0.y, x.z - x0.z} / dt;
-    V3 nw = quat_to_rotvec(qmul(d.q[i], qconj(d.q0[i]))) / dt;
+    V3 nw = quat_to_rotvec(qmul(q, qconj(d.q0[i]))) / dt;
     float sl = sqrtf(dot(nv, nv));
     if (sl > P.max_lin) nv = nv * (P.max_lin / sl);
     float sa = sqrtf(dot(nw, nw));
@@ -543,7 +605,7 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
       act = act && on;
       solve = act && (pm.it < its || post_stab);
     }
-    if (pm.finalize && valid && lane == 0) finalize_body(d, i, dt);
+    if (pm.finalize && valid && lane == 0) finalize_body(d, i, dt, xi4, d.q[i]);
     Acc s;
     acc_zero(s);
     float4 qi = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
@@ -560,7 +622,7 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
       }
       for (int k = lane; k < ns + nd; k += G) {
         int g = k < ns ? s0 + k : d.dg_idx[e0 + (k - ns)];
-        vmax = fmaxf(vmax, accumulate_group(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt));
+        vmax = fmaxf(vmax, accumulate_group<false>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt));
       }
     }
     if (G > 1) {
@@ -610,6 +672,136 @@ __device__ __forceinline__ PassMode pass_mode(const DevParams& P, int it) {
   pm.viol_slot = (P.record_violation && pm.dual && it - 1 < 64 && !P.batched) ? it - 1 : -1;
   pm.it = it;
   return pm;
+}
+
+// L1 prefetch of the group fields that no pass writes (the flag sweep reads
+// the written ones through L2).
+__device__ __forceinline__ void prefetch_group_fixed(const Dev& d, int g, bool box) {
+  prefetch_l1(d.g_meta + g);
+  prefetch_l1(d.g_ac0 + g);
+  prefetch_l1(d.g_mat + g);
+  prefetch_l1(d.g_offa + g);
+  if (box) {
+    prefetch_l1(d.g_body + g);
+    prefetch_l1(d.g_offb + g);
+    prefetch_l1(d.g_n + g);
+  }
+}
+
+// Flag-ordered sweep: all `total` passes over the colors without a grid
+// barrier.  The work is cut into chunks of W = 32/G bodies of one color of
+// one pass, numbered in (pass, color) order; warp w takes chunks w, w +
+// warps, w + 2 warps, ...  A body waits only for its own previous pass and
+// for its neighbours (lower color: this pass; higher color: the previous
+// pass), so every chunk depends only on lower-numbered chunks and the lowest
+// unfinished chunk can always run (all warps are resident).  Each body's
+// arithmetic and reduction order are those of primal_color, so the results
+// are bit-identical to the barrier sweep.
+template <int G, bool B>
+__device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize) {
+  constexpr int W = 32 / G;
+  const unsigned FULL = 0xffffffffu;
+  const DevParams& P = *d.prm;
+  const int lane = threadIdx.x & 31, slot = lane / G, gl = lane & (G - 1);
+  const int post_stab = P.post_stab;
+  const int slot_now = B ? d.ctr->slot : 0;
+  // chunks per color (colors <= 32: one lane each), inclusive prefix
+  int cnt = lane < nc ? d.color_starts[lane + 1] - d.color_starts[lane] : 0;
+  int ch = (cnt + W - 1) / W;
+  int incl = ch;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int per_pass = __shfl_sync(FULL, incl, 31);
+  const long long n_chunks = (long long)per_pass * total;
+  for (long long q = gtid >> 5; q < n_chunks; q += gsize >> 5) {
+    int it = (int)(q / per_pass), r = (int)(q - (long long)it * per_pass);
+    int c = __ffs(__ballot_sync(FULL, incl > r)) - 1;
+    int cntc = __shfl_sync(FULL, cnt, c);
+    int k = (r - __shfl_sync(FULL, incl - ch, c)) * W + slot;
+    bool valid = k < cntc;
+    int i = valid ? d.color_bodies[d.color_starts[c] + k] : 0;
+    PassMode pm = pass_mode(P, it);
+    float dt = P.dt;
+    bool act = valid && d.x0[i].w > 0.0f;  // mass is constant; x0 was written before the passes
+    bool solve = act;
+    if (B) {
+      float4 t = valid ? scene_entry(d, i) : make_float4(dt, 0.0f, 0.0f, 0.0f);
+      int its = (int)t.y;
+      dt = t.x;
+      bool on = valid && slot_now < (int)t.z && pm.it <= its;
+      pm.post = post_stab && pm.it == its;
+      pm.dual = on && pm.it >= 1;
+      pm.finalize = on && pm.it == its && its >= 1;
+      act = act && on;
+      solve = act && (pm.it < its || post_stab);
+    }
+    float4 xi4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), qi = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    if (act) {
+      wait_done(d, i, it);  // its own previous pass (possibly on another SM)
+      xi4 = __ldcg(d.x + i);
+      qi = __ldcg(d.q + i);
+    } else if (valid) {
+      xi4 = d.x[i];  // a static body: never written by the passes
+      qi = d.q[i];
+    }
+    if (pm.finalize && valid && gl == 0) finalize_body(d, i, dt, xi4, qi);
+    Acc s;
+    acc_zero(s);
+    float vmax = 0.0f, csum = 0.0f;
+    int ccnt = 0;
+    if (act) {
+      V3 xi = xyz(xi4);
+      int s0 = d.sg_start[i], ns = d.sg_start[i + 1] - s0;
+      int e0 = d.dg_start[i], nd = d.dg_start[i + 1] - e0;
+      for (int kk = gl; kk < ns + nd; kk += G) {
+        if (kk < ns) prefetch_group_fixed(d, s0 + kk, false);
+        else prefetch_group_fixed(d, d.dg_idx[e0 + (kk - ns)], true);
+      }
+      for (int kk = gl; kk < ns + nd; kk += G) {
+        int g = kk < ns ? s0 + kk : d.dg_idx[e0 + (kk - ns)];
+        vmax = fmaxf(vmax, accumulate_group<true>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt, it, c));
+      }
+    }
+    if (G > 1) {
+#pragma unroll
+      for (int o = G / 2; o > 0; o >>= 1) {
+#pragma unroll
+        for (int kk = 0; kk < 6; ++kk) {
+          s.a[kk] += __shfl_xor_sync(FULL, s.a[kk], o);
+          s.dd[kk] += __shfl_xor_sync(FULL, s.dd[kk], o);
+        }
+#pragma unroll
+        for (int kk = 0; kk < 9; ++kk) s.b[kk] += __shfl_xor_sync(FULL, s.b[kk], o);
+#pragma unroll
+        for (int kk = 0; kk < 3; ++kk) {
+          s.rl[kk] += __shfl_xor_sync(FULL, s.rl[kk], o);
+          s.ra[kk] += __shfl_xor_sync(FULL, s.ra[kk], o);
+        }
+      }
+    }
+    if (solve && gl == 0) solve_body(d, i, xi4, qi, s, dt);
+    // publish: every lane's writes (dual updates, pose, finalize) are fenced
+    // before the body's flag is released
+    __threadfence();
+    __syncwarp();
+    if (act && gl == 0) st_release(d.done + i, it + 1);
+    if (pm.viol_slot >= 0) record_violation(d, pm.viol_slot, vmax, csum, ccnt);
+  }
+}
+
+template <bool B>
+__device__ void ph_flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize) {
+  switch (d.prm->group_size) {
+    case 1: flag_sweep<1, B>(d, total, nc, gtid, gsize); break;
+    case 2: flag_sweep<2, B>(d, total, nc, gtid, gsize); break;
+    case 4: flag_sweep<4, B>(d, total, nc, gtid, gsize); break;
+    case 8: flag_sweep<8, B>(d, total, nc, gtid, gsize); break;
+    case 16: flag_sweep<16, B>(d, total, nc, gtid, gsize); break;
+    default: flag_sweep<32, B>(d, total, nc, gtid, gsize); break;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -819,9 +1011,14 @@ __device__ void ph_predict(const Dev& d, int gtid, int gsize) {
     float dt = P.dt;
     float4 x = d.x[i], q = d.q[i];
     float m = x.w;
+    // flag sweep: passes done so far; a body that never runs counts as done
+    d.done[i] = m > 0.0f ? 0 : 0x3fffffff;
     if (B) {
       float4 t = scene_entry(d, i);
-      if (!scene_on(d, t)) continue;  // the scene sits this substep out: state untouched
+      if (!scene_on(d, t)) {  // the scene sits this substep out: state untouched
+        d.done[i] = 0x3fffffff;
+        continue;
+      }
       dt = t.x;
     }
     d.x0[i] = x;
@@ -873,7 +1070,7 @@ __device__ void ph_predict(const Dev& d, int gtid, int gsize) {
 // BDF1 velocities + caps of every body (kernels_6dof.py:1871-1901).
 __device__ void ph_finalize(const Dev& d, int gtid, int gsize) {
   float dt = d.prm->dt;
-  for (int i = gtid; i < d.nb; i += gsize) finalize_body(d, i, dt);
+  for (int i = gtid; i < d.nb; i += gsize) finalize_body(d, i, dt, d.x[i], d.q[i]);
 }
 
 // Contact-cache refresh (kernels_6dof.py:2923-2995) with an epoch tag in
@@ -1216,11 +1413,17 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
   // Pass `it` applies iteration it-1's dual update inside the color passes
   // (owner-first), so each iteration is nc barriers; without a
   // post-stabilization pass the last dual and the finalize run on their own.
-  for (int it = 0; it < total; ++it) {
-    PassMode pm = pass_mode(P, it);
-    for (int c = 0; c < nc; ++c) {
-      ph_primal<BATCHED>(d, c, pm, gtid, gsize);
-      SYNC(PH_PRIMAL);
+  if (P.flag_sweep && nc > 0) {
+    // all passes at once, each body ordered against its neighbours only
+    ph_flag_sweep<BATCHED>(d, total, nc, gtid, gsize);
+    SYNC(PH_PRIMAL);
+  } else {
+    for (int it = 0; it < total; ++it) {
+      PassMode pm = pass_mode(P, it);
+      for (int c = 0; c < nc; ++c) {
+        ph_primal<BATCHED>(d, c, pm, gtid, gsize);
+        SYNC(PH_PRIMAL);
+      }
     }
   }
   if (!P.post_stab && !P.batched && iters >= 1) {

@@ -298,6 +298,9 @@ class Solver6DOF:
         self.record_violation = False
         self.blocks_per_sm = 0
         self.timing = False  # stamp the solve kernel's phases (phase_profile())
+        # persistent solve: order the color passes by per-body completion
+        # flags instead of one grid barrier per color (same results)
+        self.flag_sweep = False
         self._debug_skip_arrive = False
         self._mlp = mlp_warm_start
         self._log_new = False
@@ -672,6 +675,7 @@ class Solver6DOF:
         p.blocks_per_sm = int(self.blocks_per_sm)
         p.timing = int(self.timing)
         p.log_new_contacts = int(self._log_new)
+        p.flag_sweep = int(bool(self.flag_sweep))
         if self._scene_tab:  # the device loops cover the largest scene settings
             p.substeps = max(sc for sc, _ in self._scene_tab)
             p.iterations = max(it for _, it in self._scene_tab)

@@ -351,7 +351,7 @@ def run_gpu(args) -> None:
                    "live": {"dyn_rows": r2, "static_rows": r1, "pairs": int(st["n_pairs"]),
                             "contacts": int(st["n_dyn_groups"]), "colors": int(st["n_colors"])},
                    "launch_shape": {"group_size": s.primal_group_size, "blocks_per_sm": s.blocks_per_sm,
-                                    "autotuned": tuned is not None},
+                                    "flag_sweep": bool(s.flag_sweep), "autotuned": tuned is not None},
                    "scene_build_s": round(t_build, 2)},
         "roofline": {"bound": "hbm", "kernel": "k_solve_persistent", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -363,8 +363,9 @@ def run_gpu(args) -> None:
         "phase_ms_per_substep": {"collide": coll_ms, "solve": solve_ms},
     }
     if tuned is not None:
-        line["autotune_ms_per_frame"] = {f"G{r['group_size']}x{r['blocks_per_sm']}": round(r["ms_per_frame"], 3)
-                                         for r in tuned["table"]}
+        line["autotune_ms_per_frame"] = {
+            f"G{r['group_size']}x{r['blocks_per_sm']}{'-flags' if r['flag_sweep'] else ''}": round(r["ms_per_frame"], 3)
+            for r in tuned["table"]}
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cb = cpu_rate(steps=3, warmup=1, threads=threads, settle=60)

@@ -87,6 +87,9 @@ typedef struct AvbdParams {
   int blocks_per_sm;   /* persistent grid: CTAs per SM (0 = occupancy max) */
   int timing;          /* stamp the persistent kernel's phase boundaries */
   int log_new_contacts;/* queue the features of every new contact (training) */
+  int flag_sweep;      /* persistent solve: order the color passes by per-body
+                          completion flags (each body waits only for its own
+                          neighbours) instead of a grid barrier per color */
 } AvbdParams;
 
 typedef struct AvbdStats {
