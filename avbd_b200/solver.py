@@ -301,6 +301,8 @@ class Solver6DOF:
         # persistent solve: order the color passes by per-body completion
         # flags instead of one grid barrier per color (same results)
         self.flag_sweep = False
+        # initial dynamic-row pool (None: the reference's 192 rows per body)
+        self.dyn_row_capacity = None
         self._debug_skip_arrive = False
         self._mlp = mlp_warm_start
         self._log_new = False
@@ -448,7 +450,9 @@ class Solver6DOF:
         if self._self_collide:
             max_pairs = max(64, 16 * max(1, n))
             pc = max(256, 16 * n) if pair_cap is None else pair_cap
-            dr = max_pairs * 12 if dyn_rows is None else dyn_rows
+            # the reference's pool size (16 pairs x 12 rows per body) unless a
+            # caller sized it (dyn_row_capacity); overflow grows it either way
+            dr = (self.dyn_row_capacity or max_pairs * 12) if dyn_rows is None else dyn_rows
             hc = _next_pow2(max(1024, 8 * max_pairs))
         else:
             pc, dr, hc = 0, 0, 1024
