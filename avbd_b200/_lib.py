@@ -21,7 +21,7 @@ class AvbdDims(C.Structure):
     _fields_ = [("n_bodies", C.c_int), ("n_static_groups", C.c_int), ("n_static_rows", C.c_int),
                 ("pair_cap", C.c_int), ("dyn_row_cap", C.c_int), ("dyn_group_cap", C.c_int),
                 ("hash_cap", C.c_int), ("mlp_floats", C.c_int), ("new_cap", C.c_int),
-                ("n_scenes", C.c_int)]
+                ("n_scenes", C.c_int), ("anchor_keys", C.c_int)]
 
 
 class AvbdParams(C.Structure):
@@ -80,6 +80,7 @@ def load():
     L.avbd_read_stats.argtypes = [vp, C.POINTER(AvbdStats), vp]
     L.avbd_count_color_conflicts.argtypes = [vp, vp]
     L.avbd_cache_load.argtypes = [vp, i, vp, vp, vp]
+    L.avbd_cache_load_keys.argtypes = [vp, i, vp, vp, vp]
     L.avbd_clear_errors.argtypes = [vp, vp]
     L.avbd_step_ms.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.avbd_read_phase_marks.argtypes = [vp, vp, vp, i, vp]
@@ -93,7 +94,8 @@ def load():
     L.avbd_mlp_adam.argtypes = [vp, vp, vp, vp, i, C.c_float, C.c_float, C.c_float, C.c_float, vp]
     for name in ("avbd_layout", "avbd_create", "avbd_destroy", "avbd_set_params", "avbd_reset_state",
                  "avbd_mark_color_dirty", "avbd_substep", "avbd_step", "avbd_read_stats",
-                 "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors", "avbd_step_ms",
+                 "avbd_count_color_conflicts", "avbd_cache_load", "avbd_cache_load_keys", "avbd_clear_errors",
+                 "avbd_step_ms",
                  "avbd_read_phase_marks", "avbd_mlp_pack", "avbd_mlp_infer", "avbd_mlp_loss_grad", "avbd_mlp_adam"):
         getattr(L, name).restype = i
     _lib = L
@@ -110,7 +112,8 @@ def check(code: int, what: str) -> int:
 # Exported C symbols declared in include/avbd6.h.
 EXPORTED = ["avbd_num_arrays", "avbd_array_name", "avbd_layout", "avbd_create", "avbd_destroy",
             "avbd_set_params", "avbd_reset_state", "avbd_mark_color_dirty", "avbd_substep", "avbd_step",
-            "avbd_read_stats", "avbd_count_color_conflicts", "avbd_cache_load", "avbd_clear_errors",
+            "avbd_read_stats", "avbd_count_color_conflicts", "avbd_cache_load", "avbd_cache_load_keys",
+            "avbd_clear_errors",
             "avbd_step_ms", "avbd_read_phase_marks", "avbd_exclusive_scan_noalloc", "avbd_mlp_pack",
             "avbd_mlp_infer", "avbd_mlp_scratch_bytes", "avbd_mlp_loss_grad", "avbd_mlp_adam", "avbd_last_error"]
 

@@ -43,7 +43,8 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(H_S0, 16, H) X(H_S1, 16, H) X(SCAN_PART, 4, SP) X(SORT_HIST, 4, SH) X(C_USED, 4, N) X(C_LOST, 4, N)        \
   X(C_HIST, 4, 64 * 64) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
   X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
-  X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS) X(DONE, 4, N)
+  X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS) X(DONE, 4, N)              \
+  X(G_KEY, 8, KEYS ? G : 0)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,
@@ -60,7 +61,8 @@ const char* kNames[] = {
 bool compute_layout(const AvbdDims* dm, size_t* off, size_t* total) {
   if (!dm || dm->n_bodies < 0 || dm->n_static_groups < 0 || dm->pair_cap < 0 || dm->dyn_group_cap < 0 ||
       dm->dyn_row_cap < 0 || dm->hash_cap < 1 || (dm->hash_cap & (dm->hash_cap - 1)) != 0 ||
-      (dm->mlp_floats != 0 && dm->mlp_floats != AVBD_MLP_FLOATS) || dm->new_cap < 0 || dm->n_scenes < 0)
+      (dm->mlp_floats != 0 && dm->mlp_floats != AVBD_MLP_FLOATS) || dm->new_cap < 0 || dm->n_scenes < 0 ||
+      dm->anchor_keys < 0 || dm->anchor_keys > 1)
     return false;
   long long N = dm->n_bodies > 0 ? dm->n_bodies : 1;
   long long DG = dm->dyn_group_cap;
@@ -71,6 +73,7 @@ bool compute_layout(const AvbdDims* dm, size_t* off, size_t* total) {
   long long M = dm->mlp_floats;
   long long NC = dm->new_cap;
   long long NS = dm->n_scenes;
+  long long KEYS = dm->anchor_keys;
   long long nblk = (N + 2047) / 2048;
   long long SH = 256 * nblk + 1;
   long long big = P > SH ? P : SH;
@@ -205,6 +208,7 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.scene_of = dims->n_scenes > 0 ? PTR(const int*, SCENE_OF) : nullptr;
   d.scene_tab = dims->n_scenes > 0 ? PTR(const float4*, SCENE_TAB) : nullptr;
   d.done = PTR(int*, DONE);
+  d.g_key = dims->anchor_keys ? PTR(unsigned long long*, G_KEY) : nullptr;
   d.ctr = PTR(DevCounters*, COUNTERS);
 #undef PTR
   int occ = solve_occupancy(256, 2);
@@ -464,7 +468,15 @@ int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {
 
 int avbd_cache_load(AvbdCtx* c, int n, const int* abc, const float* state, void* stream) {
   if (!c || n < 0 || (n > 0 && (!abc || !state))) return fail(AVBD_E_INVALID, "bad cache arguments");
-  launch_cache_load(c->d, n, abc, state, (cudaStream_t)stream);
+  if (n > 0 && c->dims.anchor_keys) return fail(AVBD_E_INVALID, "anchor-keyed cache: use avbd_cache_load_keys");
+  launch_cache_load(c->d, n, abc, nullptr, state, (cudaStream_t)stream);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? AVBD_OK : fail(AVBD_E_CUDA, "cache load", e);
+}
+
+int avbd_cache_load_keys(AvbdCtx* c, int n, const unsigned long long* keys, const float* state, void* stream) {
+  if (!c || n < 0 || (n > 0 && (!keys || !state))) return fail(AVBD_E_INVALID, "bad cache arguments");
+  launch_cache_load(c->d, n, nullptr, keys, state, (cudaStream_t)stream);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? AVBD_OK : fail(AVBD_E_CUDA, "cache load", e);
 }

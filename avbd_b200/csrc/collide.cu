@@ -800,6 +800,17 @@ __global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_g
       int rs = d.pair_rstart[p], gs = d.pair_gstart[p];
       float4 nn = d.pair_nrm[p];
       int hits = 0;
+      // anchor keys: the contact point in the lower body's (ab.x) frame
+      unsigned long long akey[4] = {0ull, 0ull, 0ull, 0ull};
+      if (d.g_key) {
+        for (int c = 0; c < cnt; ++c) {
+          float4 o = d.pair_off[8 * p + (ref_is_a ? 0 : 4) + c];
+          unsigned long long k = anchor_key(ab.x, ab.y, o.x, o.y, o.z);
+          for (int c2 = 0; c2 < c; ++c2)
+            if (akey[c2] == k) k = anchor_key_rehash(k, c);
+          akey[c] = k;
+        }
+      }
       for (int c = 0; c < cnt; ++c) {
         if (rs + (c + 1) * rpc > dyn_row_cap || gs + c + 1 > dyn_group_cap) break;
         int g = d.n_sg + gs + c;
@@ -813,7 +824,9 @@ __global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_g
         float4 s0 = make_float4(0.0f, 0.0f, 0.0f, PEN_MIN);
         float4 s1 = make_float4(PEN_MIN_T, PEN_MIN_T, 0.0f, 0.0f);
         bool queued = false;
-        int slot = cache_find(d, cache_key(ab.x, ab.y, c), tag);
+        unsigned long long key = d.g_key ? akey[c] : cache_key(ab.x, ab.y, c);
+        if (d.g_key) d.g_key[g] = key;
+        int slot = cache_find(d, key, tag);
         if (slot >= 0) {
           s0 = d.h_s0[slot];
           s1 = d.h_s1[slot];

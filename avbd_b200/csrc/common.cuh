@@ -206,6 +206,8 @@ struct Dev {
   const float4* scene_tab;   // per scene: (substep dt, iterations, substeps per frame, 0)
   // flag-ordered sweep: passes each body has completed in this substep
   int* done;
+  // anchor-keyed cache (null: keys are (a, b, ordinal))
+  unsigned long long* g_key;
   // counters
   DevCounters* ctr;
 };
@@ -316,6 +318,36 @@ __host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long 
   return z;
 }
 __host__ __device__ __forceinline__ unsigned epoch_tag(unsigned epoch) { return 1u + (epoch % 16000u); }
+
+// Anchor-keyed cache (the 5 mm-quantized key of the reference's documented
+// cache, PERFORMANCE_PROGRESS.md:122-125): bodies a < b plus the contact
+// point in the body frame of a (the lower index), each coordinate rounded to
+// 5 mm, folded into a 50-bit fingerprint.  A contact keeps its warm start
+// while its anchor stays in the same 5 mm cell, whatever its ordinal in the
+// manifold.
+#define KEY_MASK50 ((1ull << 50) - 1ull)
+__host__ __device__ __forceinline__ int quant_5mm(float x) {
+#ifdef __CUDA_ARCH__
+  float s = __fmul_rn(x, 200.0f);
+  int q = __float2int_rn(s);  // round half to even
+#else
+  float s = x * 200.0f;
+  int q = (int)nearbyintf(s);
+#endif
+  return q < -32767 ? -32767 : (q > 32767 ? 32767 : q);
+}
+__host__ __device__ __forceinline__ unsigned long long anchor_key(int a, int b, float ox, float oy, float oz) {
+  unsigned long long k1 = ((unsigned long long)(unsigned)a << 32) | (unsigned long long)(unsigned)b;
+  unsigned long long k2 = ((unsigned long long)(unsigned short)(short)quant_5mm(ox) << 32) |
+                          ((unsigned long long)(unsigned short)(short)quant_5mm(oy) << 16) |
+                          (unsigned long long)(unsigned short)(short)quant_5mm(oz);
+  return mix64(k1 ^ mix64(k2 + 0x9E3779B97F4A7C15ull)) & KEY_MASK50;
+}
+// Two contacts of one pair in the same cells get distinct keys (the later
+// ordinal is rehashed), so every contact has its own cache entry.
+__host__ __device__ __forceinline__ unsigned long long anchor_key_rehash(unsigned long long k, int c) {
+  return mix64(k + (unsigned long long)(c + 1)) & KEY_MASK50;
+}
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 

@@ -23,6 +23,7 @@ int solve_occupancy(int block, int variant);
 void launch_reset(Dev& d, cudaStream_t st);
 int count_conflicts(Dev& d, cudaStream_t st);
 void launch_hash_scrub(Dev& d, cudaStream_t st);
-void launch_cache_load(Dev& d, int n, const int* abc, const float* st, cudaStream_t s);
+void launch_cache_load(Dev& d, int n, const int* abc, const unsigned long long* keys, const float* st,
+                       cudaStream_t s);
 
 }  // namespace avbd

@@ -1088,7 +1088,7 @@ __device__ void ph_collect(const Dev& d, int gtid, int gsize) {
     int meta = d.g_meta[g];
     int2 bd = d.g_body[g];
     int ka = min(bd.x, bd.y), kb = max(bd.x, bd.y);
-    unsigned long long key = cache_key(ka, kb, meta_cidx(meta));
+    unsigned long long key = d.g_key ? d.g_key[g] : cache_key(ka, kb, meta_cidx(meta));
     unsigned long long want = key | ((unsigned long long)tag << 50);
     float4 lam = d.g_lam[g], pen = d.g_pen[g];
     float4 s0, s1;
@@ -1643,12 +1643,14 @@ __global__ void k_cache_clear(const __grid_constant__ Dev d) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
   for (int s = gtid; s < d.hash_cap; s += gsize) d.h_key[s] = 0ull;
 }
-__global__ void k_cache_insert(const __grid_constant__ Dev d, int n, const int* abc, const float* st) {
+// Entries are (a, b, ordinal) triples, or raw 50-bit keys when `keys` is set.
+__global__ void k_cache_insert(const __grid_constant__ Dev d, int n, const int* abc, const unsigned long long* keys,
+                               const float* st) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
   unsigned tag = epoch_tag(d.ctr->epoch);
   unsigned mask = (unsigned)d.hash_cap - 1u;
   for (int k = gtid; k < n; k += gsize) {
-    unsigned long long key = cache_key(abc[3 * k], abc[3 * k + 1], abc[3 * k + 2]);
+    unsigned long long key = keys ? (keys[k] & KEY_MASK50) : cache_key(abc[3 * k], abc[3 * k + 1], abc[3 * k + 2]);
     unsigned long long want = key | ((unsigned long long)tag << 50);
     unsigned h = (unsigned)mix64(key) & mask;
     bool done = false;
@@ -1665,9 +1667,10 @@ __global__ void k_cache_insert(const __grid_constant__ Dev d, int n, const int* 
     if (!done) atomicOr(&d.ctr->err, ERR_HASH_FULL);
   }
 }
-void launch_cache_load(Dev& d, int n, const int* abc, const float* st, cudaStream_t s) {
+void launch_cache_load(Dev& d, int n, const int* abc, const unsigned long long* keys, const float* st,
+                       cudaStream_t s) {
   k_cache_clear<<<148 * 4, 256, 0, s>>>(d);
-  if (n > 0) k_cache_insert<<<148 * 2, 256, 0, s>>>(d, n, abc, st);
+  if (n > 0) k_cache_insert<<<148 * 2, 256, 0, s>>>(d, n, abc, keys, st);
 }
 
 }  // namespace avbd

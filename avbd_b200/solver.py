@@ -303,6 +303,7 @@ class Solver6DOF:
         self.flag_sweep = False
         # initial dynamic-row pool (None: the reference's 192 rows per body)
         self.dyn_row_capacity = None
+        self._anchor_keys = False  # cache_key_mode "anchor_5mm"
         self._debug_skip_arrive = False
         self._mlp = mlp_warm_start
         self._log_new = False
@@ -469,6 +470,7 @@ class Solver6DOF:
         # training log can use it
         d.new_cap = max(1024, 8 * n) if self._self_collide and (self._mlp is not None or self._log_new) else 0
         d.n_scenes = len(self._scene_tab)
+        d.anchor_keys = int(self._anchor_keys)
         return d
 
     def _views(self):
@@ -882,6 +884,38 @@ class Solver6DOF:
         idx = torch.as_tensor(np.asarray(gid, np.int64), device=self.device)
         return self._g_lam[idx].cpu().numpy(), self._g_pen[idx].cpu().numpy()
 
+    @property
+    def cache_key_mode(self) -> str:
+        """How the contact cache identifies a contact across substeps:
+        "ordinal" -- (a, b, place in the pair's manifold), the key of the
+        reference's live cache (kernels_6dof.py:2588-2594); "anchor_5mm" --
+        (a, b, contact point in body a's frame rounded to 5 mm), the key of
+        its documented cache (PERFORMANCE_PROGRESS.md:122-125), which
+        survives reordering of the manifold.  Changing it empties the cache."""
+        return "anchor_5mm" if self._anchor_keys else "ordinal"
+
+    @cache_key_mode.setter
+    def cache_key_mode(self, mode: str) -> None:
+        if mode not in ("ordinal", "anchor_5mm"):
+            raise ValueError(f"cache_key_mode must be 'ordinal' or 'anchor_5mm', got {mode!r}")
+        on = mode == "anchor_5mm"
+        if on != self._anchor_keys:
+            self._anchor_keys = on
+            self._dirty = True  # re-flush: the arena gains / drops the per-group key array
+
+    @property
+    def _contact_cache(self) -> dict:
+        """The warm-start contact cache as {key: state}: key (a, b, ordinal)
+        with a < b the bodies and ordinal the contact's place in the pair's
+        manifold (the raw 50-bit anchor fingerprint in "anchor_5mm" mode),
+        state 8 floats (lambda n/t1/t2, penalty n/t1/t2, was_static t1/t2).
+        A host copy of the device hash (kernels_6dof.py:2915-2995 keep the
+        same contents in hash_keys / hash_state)."""
+        sd = self.state_dict()
+        if self._anchor_keys:
+            return {int(k): st for k, st in zip(sd["cache_keys"], sd["cache_state"])}
+        return {tuple(int(v) for v in k): st for k, st in zip(sd["cache_abc"], sd["cache_state"])}
+
     @_on_stream
     def clear_contact_cache(self) -> None:
         """Empties the contact cache: every contact of the next substep is new."""
@@ -1071,14 +1105,20 @@ class Solver6DOF:
             np.int64), (k & np.uint64(3)).astype(np.int64)], axis=1).astype(np.int32) if k.size else np.zeros(
             (0, 3), np.int32)
         st = np.concatenate([self._h_s0.cpu().numpy()[live], self._h_s1.cpu().numpy()[live]], axis=1)
-        order = np.lexsort((abc[:, 2], abc[:, 1], abc[:, 0])) if k.size else np.zeros(0, np.int64)
+        raw = k & np.uint64((1 << 50) - 1)
+        if self._anchor_keys:  # fingerprints: no (a, b, ordinal) to decode
+            order = np.argsort(raw, kind="stable")
+            abc = np.zeros((0, 3), np.int32)
+        else:
+            order = np.lexsort((abc[:, 2], abc[:, 1], abc[:, 0])) if k.size else np.zeros(0, np.int64)
+            abc = abc[order]
         return dict(x=self.x[:n].cpu().numpy().astype(np.float64), q=self.q[:n].cpu().numpy().astype(np.float64),
                     v=self.v[:n].cpu().numpy().astype(np.float64), w=self.omega[:n].cpu().numpy().astype(np.float64),
                     pv=self.prev_v[:n].cpu().numpy().astype(np.float64),
                     pw=self.prev_omega[:n].cpu().numpy().astype(np.float64),
                     row_lam=lam[:ns].astype(np.float64), row_pen=pen[:ns].astype(np.float64),
                     row_active=act[:ns].copy(), row_was=was[:ns].copy(),
-                    cache_abc=abc[order], cache_state=st[order].astype(np.float64),
+                    cache_abc=abc, cache_keys=raw[order], cache_state=st[order].astype(np.float64),
                     colors=self._color[:n].cpu().numpy().copy(), n_colors=int(self._stats.n_colors),
                     color_dirty=bool(self._color_dirty))
 
@@ -1119,12 +1159,18 @@ class Solver6DOF:
             self._g_lam[:ng] = torch.from_numpy(lam).to(dev)
             self._g_pen[:ng] = torch.from_numpy(pen).to(dev)
             self._g_flags[:ng] = torch.from_numpy(fl).to(dev)
-        abc = np.ascontiguousarray(sd["cache_abc"], np.int32)
         stt = np.ascontiguousarray(sd["cache_state"], np.float32)
-        ta = torch.from_numpy(abc).to(dev) if abc.size else torch.zeros((1, 3), dtype=torch.int32, device=dev)
         ts = torch.from_numpy(stt).to(dev) if stt.size else torch.zeros((1, 8), dtype=torch.float32, device=dev)
-        _lib.check(_lib.load().avbd_cache_load(self._ctx, int(abc.shape[0]), C.c_void_p(ta.data_ptr()),
-                                               C.c_void_p(ts.data_ptr()), self._stream()), "cache_load")
+        if self._anchor_keys:
+            ks = np.ascontiguousarray(sd["cache_keys"], np.uint64).view(np.int64)
+            tk = torch.from_numpy(ks.copy()).to(dev) if ks.size else torch.zeros(1, dtype=torch.int64, device=dev)
+            _lib.check(_lib.load().avbd_cache_load_keys(self._ctx, int(ks.shape[0]), C.c_void_p(tk.data_ptr()),
+                                                        C.c_void_p(ts.data_ptr()), self._stream()), "cache_load")
+        else:
+            abc = np.ascontiguousarray(sd["cache_abc"], np.int32)
+            ta = torch.from_numpy(abc).to(dev) if abc.size else torch.zeros((1, 3), dtype=torch.int32, device=dev)
+            _lib.check(_lib.load().avbd_cache_load(self._ctx, int(abc.shape[0]), C.c_void_p(ta.data_ptr()),
+                                                   C.c_void_p(ts.data_ptr()), self._stream()), "cache_load")
         colors = np.asarray(sd["colors"], np.int32)
         self._color[:n] = torch.from_numpy(colors).to(dev)
         cs = np.zeros(64, np.int32)

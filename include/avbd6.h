@@ -62,6 +62,9 @@ typedef struct AvbdDims {
                           substeps per frame, 0) as float4; bodies of
                           different scenes never collide.  AvbdParams then
                           gives the maximum iterations and substeps. */
+  int anchor_keys;     /* contact-cache key: 0 = (a, b, manifold ordinal) as
+                          the reference's live cache; 1 = (a, b, contact point
+                          in a's frame at 5 mm) as its documented cache */
 } AvbdDims;
 
 /* Scalars of Solver6DOF.__init__ (solver_6dof.py:180-201). */
@@ -154,6 +157,11 @@ int avbd_count_color_conflicts(AvbdCtx* ctx, void* stream);
  * The reference keeps this state in hash_keys/hash_state
  * (solver_6dof.py:1150-1156, kernels_6dof.py:2923-2995). */
 int avbd_cache_load(AvbdCtx* ctx, int n, const int* abc, const float* state, void* stream);
+
+/* The same with the cache's raw 50-bit keys (bits 50-63 ignored): the only
+ * form for an anchor-keyed cache (AvbdDims.anchor_keys = 1), any cache's keys
+ * as read back from the arena's H_KEY. */
+int avbd_cache_load_keys(AvbdCtx* ctx, int n, const unsigned long long* keys, const float* state, void* stream);
 
 /* Clears the sticky device error bits. */
 int avbd_clear_errors(AvbdCtx* ctx, void* stream);

@@ -427,6 +427,32 @@ static inline uint64_t pair_key(int a, int b, int c) {
   return ((uint64_t)(uint32_t)a << 26) | ((uint64_t)(uint32_t)b << 2) | (uint64_t)c;
 }
 
+// The 5 mm anchor key (documented cache of the reference,
+// PERFORMANCE_PROGRESS.md:122-125): bodies a < b and the contact point in
+// a's body frame rounded to 5 mm (round half to even), folded into 50 bits
+// with a 64-bit finalizer; a later contact of the same pair in the same
+// cells is rehashed with its ordinal.  Same arithmetic as the device.
+static inline uint64_t mix64(uint64_t z) {
+  z ^= z >> 31;
+  z *= 0x7fb5d329728ea185ull;
+  z ^= z >> 27;
+  z *= 0x81dadef4bc2dd44dull;
+  z ^= z >> 33;
+  return z;
+}
+static inline int quant_5mm(float x) {
+  float s = x * 200.0f;
+  int q = (int)std::nearbyint(s);
+  return q < -32767 ? -32767 : (q > 32767 ? 32767 : q);
+}
+static const uint64_t KEY_MASK50 = (1ull << 50) - 1ull;
+static inline uint64_t anchor_key(int a, int b, V3<float> o) {
+  uint64_t k1 = ((uint64_t)(uint32_t)a << 32) | (uint64_t)(uint32_t)b;
+  uint64_t k2 = ((uint64_t)(uint16_t)(int16_t)quant_5mm(o.x) << 32) | ((uint64_t)(uint16_t)(int16_t)quant_5mm(o.y) << 16) |
+                (uint64_t)(uint16_t)(int16_t)quant_5mm(o.z);
+  return mix64(k1 ^ mix64(k2 + 0x9E3779B97F4A7C15ull)) & KEY_MASK50;
+}
+
 // ---------------------------------------------------------------------------
 // The simulation state.
 // ---------------------------------------------------------------------------
@@ -468,7 +494,8 @@ template <class R> struct Sim {
   // contact cache
   struct Entry { R s[8]; };
   std::unordered_map<uint64_t, Entry> cache;
-  struct Pool { int n, t, b, c; };
+  struct Pool { int n, t, b, c; uint64_t key; };
+  int key_mode = 0;  // 0: (a, b, ordinal) keys; 1: 5 mm anchor keys
   std::vector<Pool> pool;
 
   // coloring
@@ -551,6 +578,17 @@ template <class R> struct Sim {
       if (mr > 0.0f || mi > 0.0f) m = std::sqrt(mr * mi);
       float ms = m * fsm;
       int ka = std::min(ref, inc), kb = std::max(ref, inc);
+      uint64_t keys[4];
+      for (int c = 0; c < o.count; ++c) {
+        if (key_mode) {
+          uint64_t k = anchor_key(ka, kb, ka == ref ? o.off_ref[c] : o.off_inc[c]);
+          for (int c2 = 0; c2 < c; ++c2)
+            if (keys[c2] == k) k = mix64(k + (uint64_t)(c + 1)) & KEY_MASK50;
+          keys[c] = k;
+        } else {
+          keys[c] = pair_key(ka, kb, c);
+        }
+      }
       for (int c = 0; c < o.count; ++c) {
         int rpc = m <= 0.0f ? 1 : 3;
         long long base = nr;
@@ -571,13 +609,13 @@ template <class R> struct Sim {
           setrow(b, TANGENT, o.bb, -FINF, FINF, n, t, m, ms);
         }
         R s[8] = {0, 0, 0, R(PEN_MIN), R(PEN_MIN_T), R(PEN_MIN_T), 0, 0};
-        auto it = cache.find(pair_key(ka, kb, c));
+        auto it = cache.find(keys[c]);
         if (it != cache.end())
           for (int k = 0; k < 8; ++k) s[k] = it->second.s[k];
         lam[n] = s[0]; pen[n] = s[3]; was[n] = 0;
         if (t >= 0) { lam[t] = s[1]; pen[t] = s[4]; was[t] = (int)s[6]; }
         if (b >= 0) { lam[b] = s[2]; pen[b] = s[5]; was[b] = (int)s[7]; }
-        pool.push_back({n, t, b, c});
+        pool.push_back({n, t, b, c, keys[c]});
       }
     }
     n_rows_reserved = nr;
@@ -966,14 +1004,12 @@ template <class R> struct Sim {
     cache.clear();
     for (const Pool& p : pool) {
       if (!active[p.n]) continue;
-      int a = ba[p.n], b = bb[p.n];
-      int ka = std::min(a, b), kb = std::max(a, b);
       Entry e;
       e.s[0] = lam[p.n]; e.s[3] = pen[p.n];
       e.s[1] = 0; e.s[2] = 0; e.s[4] = R(PEN_MIN_T); e.s[5] = R(PEN_MIN_T); e.s[6] = 0; e.s[7] = 0;
       if (p.t >= 0) { e.s[1] = lam[p.t]; e.s[4] = pen[p.t]; e.s[6] = (R)was[p.t]; }
       if (p.b >= 0) { e.s[2] = lam[p.b]; e.s[5] = pen[p.b]; e.s[7] = (R)was[p.b]; }
-      cache[pair_key(ka, kb, p.c)] = e;
+      cache[p.key] = e;
     }
   }
 
@@ -1219,6 +1255,40 @@ int orc_set_static_rows(void* p, const double* lam, const double* pen, const int
   });
 }
 // Contact cache: keys (a, b, c) as int triples and 8 state values each.
+int orc_set_key_mode(void* p, int mode) {
+  return dispatch((OrcHandle*)p, [&](auto& s) {
+    s.key_mode = mode ? 1 : 0;
+    s.cache.clear();
+    return 0;
+  });
+}
+// Contact cache as raw keys (either mode) and 8 state values each, keys sorted.
+int orc_get_cache_keys(void* p, int cap, uint64_t* keys, double* st) {
+  return dispatch((OrcHandle*)p, [&](auto& s) {
+    std::vector<uint64_t> ks;
+    for (auto& kv : s.cache) ks.push_back(kv.first);
+    std::sort(ks.begin(), ks.end());
+    int n = (int)ks.size();
+    for (int k = 0; k < n && k < cap; ++k) {
+      keys[k] = ks[k];
+      const auto& e = s.cache[ks[k]];
+      for (int u = 0; u < 8; ++u) st[8 * k + u] = e.s[u];
+    }
+    return n;
+  });
+}
+int orc_set_cache_keys(void* p, int n, const uint64_t* keys, const double* st) {
+  return dispatch((OrcHandle*)p, [&](auto& s) {
+    using R = std::remove_reference_t<decltype(s.dt)>;
+    s.cache.clear();
+    for (int k = 0; k < n; ++k) {
+      typename std::remove_reference_t<decltype(s)>::Entry e;
+      for (int u = 0; u < 8; ++u) e.s[u] = (R)st[8 * k + u];
+      s.cache[keys[k] & KEY_MASK50] = e;
+    }
+    return 0;
+  });
+}
 int orc_get_cache(void* p, int cap, int* abc, double* st) {
   return dispatch((OrcHandle*)p, [&](auto& s) {
     std::vector<uint64_t> ks;

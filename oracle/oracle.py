@@ -59,6 +59,9 @@ def lib():
         L.orc_set_static_rows.argtypes = [vp] * 5
         L.orc_get_cache.argtypes = [vp, i, vp, vp]
         L.orc_set_cache.argtypes = [vp, i, vp, vp]
+        L.orc_set_key_mode.argtypes = [vp, i]
+        L.orc_get_cache_keys.argtypes = [vp, i, vp, vp]
+        L.orc_set_cache_keys.argtypes = [vp, i, vp, vp]
         L.orc_get_colors.argtypes = [vp, vp]
         L.orc_set_colors.argtypes = [vp, vp, i, i]
         L.orc_get_pairs.argtypes = [vp, i] + [vp] * 6
@@ -403,6 +406,23 @@ class OracleSolver6DOF:
         st = np.zeros((cap, 8))
         n = lib().orc_get_cache(self._h, cap, _p(abc), _p(st))
         return abc[:n].copy(), st[:n].copy()
+
+    def set_key_mode(self, mode: str) -> None:
+        """'ordinal' (a, b, manifold ordinal) or 'anchor_5mm' cache keys;
+        empties the cache."""
+        lib().orc_set_key_mode(self._h, 1 if mode == "anchor_5mm" else 0)
+
+    def cache_keys(self):
+        cap = 1 << 22
+        keys = np.zeros(cap, np.uint64)
+        st = np.zeros((cap, 8))
+        n = lib().orc_get_cache_keys(self._h, cap, _p(keys), _p(st))
+        return keys[:n].copy(), st[:n].copy()
+
+    def set_cache_keys(self, keys, st):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        st = np.ascontiguousarray(st, np.float64)
+        lib().orc_set_cache_keys(self._h, keys.shape[0], _p(keys), _p(st))
 
     def set_cache(self, abc, st):
         abc = np.ascontiguousarray(abc, np.int32)

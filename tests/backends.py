@@ -38,6 +38,9 @@ def sync_oracle_from_gpu(sg, so):
     sd = sg.state_dict()
     so.set_bodies(sd["x"], sd["q"], sd["v"], sd["w"], sd["pv"], sd["pw"])
     so.set_static_rows(sd["row_lam"], sd["row_pen"], sd["row_active"], sd["row_was"])
-    so.set_cache(sd["cache_abc"], sd["cache_state"])
+    if sg.cache_key_mode == "anchor_5mm":
+        so.set_cache_keys(sd["cache_keys"], sd["cache_state"])
+    else:
+        so.set_cache(sd["cache_abc"], sd["cache_state"])
     so.set_colors(sd["colors"], sd["n_colors"], sd["color_dirty"])
     return sd
