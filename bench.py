@@ -237,6 +237,8 @@ def run_gpu(args) -> None:
     dev = torch.device("cuda", local)
     size = dict(FULL) if not args.small else dict(nx=40, nz=40, ny=10)
     s = Solver6DOF(device=str(dev), **PARAMS)
+    if args.row_capacity:
+        s.dyn_row_capacity = args.row_capacity  # smaller arena for profiler captures
     if args.group_size:
         s.primal_group_size = args.group_size
     if args.blocks_per_sm:
@@ -479,6 +481,7 @@ def main():
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="solve CTAs per SM (0 = autotuned)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start evaluation")
+    ap.add_argument("--row-capacity", type=int, default=0, help="initial dynamic-row pool (0 = reference size)")
     ap.add_argument("--batched", action="store_true", help="512 batched scenes vs one scene at a time")
     ap.add_argument("--seq-scenes", type=int, default=64, help="scenes in the one-at-a-time comparison")
     ap.add_argument("--settle-batched", type=int, default=60)
