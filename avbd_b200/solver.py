@@ -1031,6 +1031,24 @@ class Solver6DOF:
     def active(self) -> np.ndarray:
         return self._row_state()[3]
 
+    @property
+    def stream(self) -> torch.cuda.Stream:
+        """The CUDA stream every launch of this solver is enqueued on."""
+        return self._cuda_stream
+
+    def state_views(self) -> dict:
+        """Zero-copy device views of the body state (torch tensors on the
+        solver's device, valid until the scene is rebuilt): positions [N, 3],
+        orientations [N, 4] (xyzw), velocities [N, 3], angular_velocities
+        [N, 3].  The host-copy getters and read_state_batched
+        (solver_6dof.py:1920-2052) stay available; consumers on another
+        stream wait on `stream` before reading.  Writes through the views
+        change the simulation."""
+        self._flush()
+        n = len(self._x)
+        return {"positions": self.x[:n], "orientations": self.q[:n], "velocities": self.v[:n],
+                "angular_velocities": self.omega[:n]}
+
     def read_state_batched(self, include_rows: bool = True) -> dict:
         """Positions, orientations, angular velocities and per-row diagnostics
         (solver_6dof.py:1952-2052)."""

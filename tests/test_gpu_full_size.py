@@ -80,3 +80,14 @@ def test_full_size_substep_is_bit_reproducible(pile):
         out.append(pile.state_dict())
     for k in ("x", "q", "v", "w", "cache_state"):
         np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
+
+
+def test_zero_copy_state_views(pile):
+    v = pile.state_views()
+    pile.stream.synchronize()
+    np.testing.assert_array_equal(v["positions"].cpu().numpy(), pile.positions().astype(np.float32))
+    np.testing.assert_array_equal(v["orientations"].cpu().numpy(), pile.orientations().astype(np.float32))
+    assert v["positions"].data_ptr() == pile.x4.data_ptr()  # a view of the arena, not a copy
+    pile.step()  # the same views follow the state
+    pile.stream.synchronize()
+    np.testing.assert_array_equal(v["positions"].cpu().numpy(), pile.positions().astype(np.float32))
