@@ -370,7 +370,10 @@ def run_gpu(args) -> None:
             for r in tuned["table"]}
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cb = cpu_rate(steps=3, warmup=1, threads=threads, settle=60)
+        # the same sample as the reference arm: a settled tile (fewer settle
+        # frames would time a tile whose boxes are still falling, with a
+        # third of the contact rows)
+        cb = cpu_rate(steps=3, warmup=3, threads=threads, settle=120)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0 and not args.no_warm_start:
         line["warm_start"] = warm_start_eval()
