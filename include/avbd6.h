@@ -87,7 +87,8 @@ typedef struct AvbdParams {
   int record_violation;/* store the max constraint violation per iteration */
   int mlp_warm_start;  /* 1 = learned warm start for new contacts */
   int debug_skip_arrive; /* test hook: block 0 skips one barrier arrival */
-  int blocks_per_sm;   /* persistent grid: CTAs per SM (0 = occupancy max) */
+  int blocks_per_sm;   /* persistent grid: CTAs per SM, 2 or 3, each with its
+                          own register budget (128 / 80 registers); 0 = 2 */
   int timing;          /* stamp the persistent kernel's phase boundaries */
   int log_new_contacts;/* queue the features of every new contact (training) */
   int flag_sweep;      /* persistent solve: order the color passes by per-body
