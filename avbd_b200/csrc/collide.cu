@@ -380,22 +380,47 @@ __device__ __forceinline__ void bvh_query_upper(const Dev& d, int i, F fn) {
   float4 lo = d.aabb_lo[i], hi = d.aabb_hi[i];
   bool si = d.x[i].w <= 0.0f;
   int sc = d.scene_of ? d.scene_of[i] : 0;  // batched scenes never collide with each other
+  auto leaf = [&](int node) {
+    int j = d.order[node - (n - 1)];
+    if (j > i && !(si && d.x[j].w <= 0.0f) && (!d.scene_of || d.scene_of[j] == sc)) fn(j);
+  };
+  if (!overlap(lo, hi, d.node_lo[0], d.node_hi[0])) return;
+  if (n - 1 <= 0) {  // a single body: the root is its leaf
+    leaf(0);
+    return;
+  }
+  // Children are tested before they are pushed: overlapping leaves are
+  // reported at once, a single overlapping inner child is descended into
+  // directly, and only the second of two is pushed.
   int stack[64];
   int sp = 0;
-  stack[sp++] = 0;
-  while (sp > 0) {
-    int node = stack[--sp];
-    if (!overlap(lo, hi, d.node_lo[node], d.node_hi[node])) continue;
-    if (node >= n - 1) {
-      int j = d.order[node - (n - 1)];
-      if (j > i && !(si && d.x[j].w <= 0.0f) && (!d.scene_of || d.scene_of[j] == sc)) fn(j);
-    } else {
-      if (sp + 2 > 64) {
+  int node = 0;
+  while (true) {
+    int l = d.node_left[node], r = d.node_right[node];
+    bool ol = overlap(lo, hi, d.node_lo[l], d.node_hi[l]);
+    bool orr = overlap(lo, hi, d.node_lo[r], d.node_hi[r]);
+    if (ol && l >= n - 1) {
+      leaf(l);
+      ol = false;
+    }
+    if (orr && r >= n - 1) {
+      leaf(r);
+      orr = false;
+    }
+    if (ol && orr) {
+      if (sp + 1 > 64) {
         atomicOr(&d.ctr->err, ERR_BVH);
         return;
       }
-      stack[sp++] = d.node_left[node];
-      stack[sp++] = d.node_right[node];
+      stack[sp++] = r;
+      node = l;
+    } else if (ol) {
+      node = l;
+    } else if (orr) {
+      node = r;
+    } else {
+      if (sp == 0) break;
+      node = stack[--sp];
     }
   }
 }
