@@ -45,6 +45,7 @@ __global__ void k_begin_substep(const __grid_constant__ Dev d) {
     c->n_mlp_applied = 0;
     c->n_mlp_fallback = 0;
     c->n_mlp_reverted = 0;
+    for (int k = 0; k < 4; ++k) c->work_ctr[k] = 0;
     c->slot = c->slot_next;  // substep slot within the frame (batched scenes)
     c->slot_next = c->slot + 1;
     c->max_dg = 0;

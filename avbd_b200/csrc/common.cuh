@@ -117,7 +117,8 @@ struct DevCounters {
   unsigned pad3[31];
   unsigned bar_sub[16][32];
   int round_unc[2];  // uncolored counts of alternate coloring rounds
-  int pad4[30];
+  int work_ctr[4];   // color passes: next chunk to hand out (pass q uses q & 3)
+  int pad4[26];
   float vc_sum[64];  // per-iteration violation sum over box-box contact groups
   int vc_cnt[64];    // and their count (record_violation)
 };

@@ -574,18 +574,26 @@ __device__ __forceinline__ void record_violation(const Dev& d, int slot, float v
 
 // Primal sweep of one color: G lanes per body, butterfly reduction of the
 // 27 accumulators, lane 0 solves (kernels_6dof.py:1149-1414, in place).
+//
+// Work is dealt in chunks of 32/G bodies, one chunk per warp: every warp
+// starts on chunk (its warp index), and a warp that finishes takes the next
+// undealt chunk from the pass's counter (heavy bodies come first in each
+// color, so the light ones fill in behind them and the pass ends sooner than
+// with a fixed stride).  Which warp runs a body never changes its result.
 template <int G, bool B>
-__device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gtid, int gsize) {
+__device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gtid, int gsize, int pass) {
+  constexpr int W = 32 / G;
   const int post_stab = d.prm->post_stab;
   const int slot_now = B ? d.ctr->slot : 0;
   int cs0 = d.color_starts[c];
   int nbody = d.color_starts[c + 1] - cs0;
-  int total = nbody * G;
+  const int nchunks = (nbody + W - 1) / W, nwarps = gsize >> 5;
+  int* counter = &d.ctr->work_ctr[pass & 3];
+  if (gtid == 0) d.ctr->work_ctr[(pass + 2) & 3] = 0;  // two passes ahead: no warp touches it now
   float vmax = 0.0f, csum = 0.0f;
   int ccnt = 0;
-  for (int base = 0; base < total; base += gsize) {
-    int t = base + gtid;
-    int slot = t / G, lane = t & (G - 1);
+  for (int chunk = gtid >> 5; chunk < nchunks;) {
+    int slot = chunk * W + (threadIdx.x & 31) / G, lane = threadIdx.x & (G - 1);
     bool valid = slot < nbody;
     int i = valid ? d.color_bodies[cs0 + slot] : 0;
     float4 xi4 = valid ? d.x[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -643,6 +651,9 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
       }
     }
     if (solve && lane == 0) solve_body(d, i, xi4, qi, s, dt);
+    int next = 0;
+    if ((threadIdx.x & 31) == 0) next = nwarps + atomicAdd(counter, 1);
+    chunk = __shfl_sync(0xffffffffu, next, 0);
   }
   if (pm.viol_slot >= 0) record_violation(d, pm.viol_slot, vmax, csum, ccnt);
 }
@@ -650,15 +661,15 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
 // B: batched scenes (a separate instantiation, so the single-scene sweep's
 // register allocation does not carry the per-scene state).
 template <bool B>
-__device__ void ph_primal(const Dev& d, int c, PassMode pm, int gtid, int gsize) {
+__device__ void ph_primal(const Dev& d, int c, PassMode pm, int gtid, int gsize, int pass) {
   float dt = d.prm->dt;
   switch (d.prm->group_size) {
-    case 1: primal_color<1, B>(d, c, pm, dt, gtid, gsize); break;
-    case 2: primal_color<2, B>(d, c, pm, dt, gtid, gsize); break;
-    case 4: primal_color<4, B>(d, c, pm, dt, gtid, gsize); break;
-    case 8: primal_color<8, B>(d, c, pm, dt, gtid, gsize); break;
-    case 16: primal_color<16, B>(d, c, pm, dt, gtid, gsize); break;
-    default: primal_color<32, B>(d, c, pm, dt, gtid, gsize); break;
+    case 1: primal_color<1, B>(d, c, pm, dt, gtid, gsize, pass); break;
+    case 2: primal_color<2, B>(d, c, pm, dt, gtid, gsize, pass); break;
+    case 4: primal_color<4, B>(d, c, pm, dt, gtid, gsize, pass); break;
+    case 8: primal_color<8, B>(d, c, pm, dt, gtid, gsize, pass); break;
+    case 16: primal_color<16, B>(d, c, pm, dt, gtid, gsize, pass); break;
+    default: primal_color<32, B>(d, c, pm, dt, gtid, gsize, pass); break;
   }
 }
 
@@ -1421,7 +1432,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
     for (int it = 0; it < total; ++it) {
       PassMode pm = pass_mode(P, it);
       for (int c = 0; c < nc; ++c) {
-        ph_primal<BATCHED>(d, c, pm, gtid, gsize);
+        ph_primal<BATCHED>(d, c, pm, gtid, gsize, it * nc + c);
         SYNC(PH_PRIMAL);
       }
     }
@@ -1504,8 +1515,9 @@ __global__ void ks_predict(const __grid_constant__ Dev d) {
 __global__ void ks_primal(const __grid_constant__ Dev d, int it, int c) {
   GS;
   if (c >= d.ctr->n_colors) return;
-  if (d.prm->batched) ph_primal<true>(d, c, pass_mode(*d.prm, it), gtid, gsize);
-  else ph_primal<false>(d, c, pass_mode(*d.prm, it), gtid, gsize);
+  int pass = it * d.ctr->n_colors + c;
+  if (d.prm->batched) ph_primal<true>(d, c, pass_mode(*d.prm, it), gtid, gsize, pass);
+  else ph_primal<false>(d, c, pass_mode(*d.prm, it), gtid, gsize, pass);
 }
 __global__ void ks_tail(const __grid_constant__ Dev d) {
   GS;
