@@ -9,7 +9,9 @@ Three knobs decide how the persistent solve kernel maps onto the 148 SMs:
   register budget, 128 or 80 registers per thread);
 * how the color passes are ordered: a grid barrier per color, or per-body
   completion flags (each body waits only for its neighbours, so passes of
-  small colors overlap).
+  small colors overlap);
+* with barriers, whether colors too small to fill the resident warps get
+  more lanes per body (`adaptive_lanes`).
 
 The best pair depends on the scene: bodies per color, groups per body and
 whether the group records fit in L2.  `autotune` times every candidate on the
@@ -43,29 +45,30 @@ def _time_frames(solver, frames: int, warm: int) -> float:
     return ms / frames
 
 
-def autotune(solver, group_sizes=(4, 8, 16), blocks_per_sm=(2, 3), flag_sweep=(False, True), frames: int = 2,
-             warm: int = 1, apply: bool = True) -> dict:
-    """Times each (group size, CTAs per SM, sweep ordering) candidate for
-    `frames` frames and returns {"best": {...}, "table": [...]}; sets the
-    best candidate on the solver when `apply`.  The scene state is restored
-    afterwards."""
+def autotune(solver, group_sizes=(4, 8, 16), blocks_per_sm=(2, 3), flag_sweep=(False, True),
+             adaptive_lanes=(False, True), frames: int = 2, warm: int = 1, apply: bool = True) -> dict:
+    """Times each (group size, CTAs per SM, sweep ordering, adaptive lanes)
+    candidate for `frames` frames and returns {"best": {...}, "table":
+    [...]}; sets the best candidate on the solver when `apply`.  Adaptive
+    lanes only apply to the barrier sweep, so flag-sweep candidates are timed
+    without them.  The scene state is restored afterwards."""
     solver._flush()
     sd = solver.state_dict()
-    g0, b0, f0 = solver.primal_group_size, solver.blocks_per_sm, solver.flag_sweep
+    knobs = ("primal_group_size", "blocks_per_sm", "flag_sweep", "adaptive_lanes")
+    keep = [getattr(solver, k) for k in knobs]
     table = []
-    for g, b, f in itertools.product(group_sizes, blocks_per_sm, flag_sweep):
+    for g, b, f, a in itertools.product(group_sizes, blocks_per_sm, flag_sweep, adaptive_lanes):
+        if f and a:
+            continue
         solver.load_state_dict(sd)
-        solver.primal_group_size = g
-        solver.blocks_per_sm = b
-        solver.flag_sweep = f
-        table.append({"group_size": g, "blocks_per_sm": b, "flag_sweep": f,
+        for k, v in zip(knobs, (g, b, f, a)):
+            setattr(solver, k, v)
+        table.append({"group_size": g, "blocks_per_sm": b, "flag_sweep": f, "adaptive_lanes": a,
                       "ms_per_frame": _time_frames(solver, frames, warm)})
     best = min(table, key=lambda r: r["ms_per_frame"])
     solver.load_state_dict(sd)
-    if apply:
-        solver.primal_group_size = best["group_size"]
-        solver.blocks_per_sm = best["blocks_per_sm"]
-        solver.flag_sweep = best["flag_sweep"]
-    else:
-        solver.primal_group_size, solver.blocks_per_sm, solver.flag_sweep = g0, b0, f0
+    chosen = ([best["group_size"], best["blocks_per_sm"], best["flag_sweep"], best["adaptive_lanes"]]
+              if apply else keep)
+    for k, v in zip(knobs, chosen):
+        setattr(solver, k, v)
     return {"best": best, "table": table}

@@ -266,6 +266,7 @@ static void fill_devparams(AvbdCtx* c, float dt_sub) {
   q.log_new = P.log_new_contacts && c->dims.new_cap > 0;
   q.batched = c->dims.n_scenes > 0;
   q.flag_sweep = P.flag_sweep;
+  q.adaptive_lanes = P.adaptive_lanes;
   q.barrier_timeout_ns = P.debug_skip_arrive ? 200000000ull : 2000000000ull;
   q.timing = P.timing;
 }

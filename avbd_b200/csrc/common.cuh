@@ -146,7 +146,8 @@ struct DevParams {
   int log_new;  // queue every new contact's features (training-data log)
   int batched;  // bodies belong to scenes with their own dt / iterations / substeps
   int flag_sweep;  // color passes ordered by per-body completion flags instead of grid barriers
-  int pad[4];
+  int adaptive_lanes;  // small colors get more lanes per body (barrier sweep)
+  int pad[3];
 };
 
 // Phase ids of the persistent kernel's timestamps.

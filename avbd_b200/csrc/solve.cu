@@ -660,10 +660,24 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
 
 // B: batched scenes (a separate instantiation, so the single-scene sweep's
 // register allocation does not carry the per-scene state).
+//
+// adaptive_lanes: a pass's time has a floor of one chunk's chain of
+// dependent loads, so a color too small to fill the resident warps runs
+// faster with more lanes per body (fewer groups per lane): the lane count
+// doubles while the color, at twice the lanes, still fits in one round of
+// the resident warps.  Only
+// the order of the per-body sums changes; the choice depends on the color's
+// size alone, so runs stay reproducible.
 template <bool B>
 __device__ void ph_primal(const Dev& d, int c, PassMode pm, int gtid, int gsize, int pass) {
   float dt = d.prm->dt;
-  switch (d.prm->group_size) {
+  int lanes = d.prm->group_size;
+  if (d.prm->adaptive_lanes) {
+    long long nbody = d.color_starts[c + 1] - d.color_starts[c];
+    long long warp_lanes = (long long)(gsize >> 5) * 32;  // lanes of one round of the resident warps
+    while (lanes < 32 && nbody * (2 * lanes) <= warp_lanes) lanes *= 2;
+  }
+  switch (lanes) {
     case 1: primal_color<1, B>(d, c, pm, dt, gtid, gsize, pass); break;
     case 2: primal_color<2, B>(d, c, pm, dt, gtid, gsize, pass); break;
     case 4: primal_color<4, B>(d, c, pm, dt, gtid, gsize, pass); break;
@@ -1247,6 +1261,132 @@ __device__ void ph_resolve_apply(const Dev& d, int* unc_out, int gtid, int gsize
   if (lane_id() == 0 && unc) atomicAdd(unc_out, unc);
 }
 
+// Jones-Plassmann as one dataflow phase (persistent kernel only: it needs
+// every thread of the grid resident).  A JP round colors a body once every
+// higher-priority neighbour is colored, with the smallest color none of them
+// holds, so the result is the greedy coloring in decreasing priority, and the
+// round that colors body i is r(i) = 1 + max r over its higher-priority
+// neighbours (0 with none).  A body with r(i) >= JP_ROUNDS is still
+// uncolored after the last round and the bucket phase gives it color 0.
+// Here each body publishes st[i] = 1 + 64 r(i) + color (color 63 =
+// uncolored) once all its higher-priority neighbours have published: the
+// same colors as the round loop, without its 2 x JP_ROUNDS grid barriers.
+// The published word is the only data exchanged, so plain relaxed loads
+// and stores suffice.  Neighbours are the other bodies of the body's contact
+// groups (the kept-pair graph of the round loop; a pair's groups are
+// adjacent in the sorted incidence list, so repeats are adjacent too).
+//
+// Progress: a thread takes its bodies (gtid, gtid + gsize, ...) in
+// decreasing priority.  For the current body it collects up to DF_HP
+// higher-priority neighbours, polls all of them at once, and never waits
+// inside a step.  The highest-priority body not yet published is its
+// thread's current body, and everything it waits for has published, so it
+// always advances.  Returns false (nothing done) when a thread would hold
+// more than 32 bodies; the caller then runs the round loop.
+#define DF_HP 8
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __noinline__ bool ph_color_dataflow(const Dev& d, int gtid, int gsize) {
+  const int nb = d.nb;
+  if ((long long)nb > 32LL * gsize) return false;
+  int* st = d.c_lost;  // zeroed by ph_color_reset
+  int nk = gtid < nb ? (nb - 1 - gtid) / gsize + 1 : 0;
+  unsigned todo = nk >= 32 ? 0xffffffffu : ((1u << nk) - 1u);
+  int cur = -1, kp = 0, ke = 0, rmax = -1, last = -1, pending = 0;
+  float pcur = 0.0f;
+  unsigned used = 0;
+  int hp[DF_HP];
+  auto take_next = [&]() {
+    cur = -1;
+    for (unsigned m = todo; m; m &= m - 1) {
+      int j = gtid + (__ffs(m) - 1) * gsize;
+      float pj = d.prio[j];
+      if (cur < 0 || pj > pcur || (pj == pcur && j < cur)) {
+        cur = j;
+        pcur = pj;
+      }
+    }
+    if (cur >= 0) {
+      todo &= ~(1u << ((cur - gtid) / gsize));
+      kp = d.dg_start[cur];
+      ke = d.dg_start[cur + 1];
+      rmax = -1;
+      last = -1;
+      used = 0;
+    }
+  };
+  // Next batch of higher-priority neighbours into hp[0..pending).
+  auto collect = [&]() {
+#pragma unroll
+    for (int j = 0; j < DF_HP; ++j) hp[j] = -1;
+    pending = 0;
+    for (; kp < ke && pending < DF_HP; ++kp) {
+      int2 bd = d.g_body[d.dg_idx[kp]];
+      int o = bd.x == cur ? bd.y : bd.x;
+      if (o == last) continue;
+      last = o;
+      float po = d.prio[o];
+      if (!(po > pcur || (po == pcur && o < cur))) continue;
+#pragma unroll
+      for (int j = DF_HP - 1; j > 0; --j) hp[j] = hp[j - 1];  // shift: keeps hp[] in registers
+      hp[0] = o;
+      ++pending;
+    }
+  };
+  take_next();
+  unsigned long long t0 = 0;
+  const unsigned long long budget = d.prm->barrier_timeout_ns;
+  unsigned polls = 0;
+  while (cur >= 0) {
+    if (pending == 0 && kp < ke) collect();
+    if (pending > 0) {
+#pragma unroll
+      for (int j = 0; j < DF_HP; ++j) {
+        if (hp[j] < 0) continue;
+        int s = ld_relaxed(st + hp[j]);
+        if (s == 0) continue;
+        --s;
+        rmax = max(rmax, s >> 6);
+        if ((s & 63) < MAX_COLORS) used |= 1u << (s & 63);
+        hp[j] = -1;
+        --pending;
+      }
+      if (rmax + 1 >= JP_ROUNDS) {  // uncolored whatever the other neighbours hold
+        pending = 0;
+        kp = ke;
+      }
+    }
+    if (pending == 0 && kp >= ke) {
+      int r = rmax + 1, c = 63;
+      if (r >= JP_ROUNDS) {
+        r = JP_ROUNDS;
+      } else {
+        c = first_fit((int)used);
+        d.color[cur] = c;
+      }
+      asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(st + cur), "r"(1 + (r << 6) + c) : "memory");
+      take_next();
+      continue;
+    }
+    if (pending == 0) continue;  // more neighbours to collect
+    if ((++polls & 31u) == 0u) {
+      if (*(volatile int*)&d.ctr->err & ERR_BARRIER_TIMEOUT) return true;
+      unsigned long long now = gtimer();
+      if (t0 == 0) t0 = now;
+      else if (now - t0 > budget) {
+        atomicOr(&d.ctr->err, ERR_BARRIER_TIMEOUT);
+        return true;
+      }
+    }
+    __nanosleep(32);
+  }
+  return true;
+}
+
 // Bucketing of bodies by color.  Within a color, bodies with many incident
 // groups come first (the longest jobs start in the first wave of a pass),
 // then by body index; deterministic.  Key = 2 * color + (light ? 1 : 0).
@@ -1387,10 +1527,12 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
     bool jp = P.color_mode == 1;
     ph_color_reset(d, gtid, gsize);
     SYNC(PH_COLOR_RESET);
+    bool dataflow = jp && ph_color_dataflow(d, gtid, gsize);
+    if (dataflow) SYNC(PH_ROUND);
     // Round r counts its uncolored bodies into round_unc[r & 1]; every block
     // reads it after the round's last barrier.  The other slot is cleared
     // during round r's second phase, when all blocks have read it.
-    int rounds = jp ? JP_ROUNDS : MAX_COLORS;
+    int rounds = dataflow ? 0 : (jp ? JP_ROUNDS : MAX_COLORS);
     for (int r = 0; r < rounds; ++r) {
       int* unc_slot = &d.ctr->round_unc[r & 1];
       ph_round_edges(d, jp, gtid, gsize);

@@ -301,6 +301,7 @@ class Solver6DOF:
         # persistent solve: order the color passes by per-body completion
         # flags instead of one grid barrier per color (same results)
         self.flag_sweep = False
+        self.adaptive_lanes = False  # more lanes per body for small colors (barrier sweep)
         # initial dynamic-row pool (None: the reference's 192 rows per body)
         self.dyn_row_capacity = None
         self._anchor_keys = False  # cache_key_mode "anchor_5mm"
@@ -682,6 +683,7 @@ class Solver6DOF:
         p.timing = int(self.timing)
         p.log_new_contacts = int(self._log_new)
         p.flag_sweep = int(bool(self.flag_sweep))
+        p.adaptive_lanes = int(bool(self.adaptive_lanes))
         if self._scene_tab:  # the device loops cover the largest scene settings
             p.substeps = max(sc for sc, _ in self._scene_tab)
             p.iterations = max(it for _, it in self._scene_tab)

@@ -353,7 +353,8 @@ def run_gpu(args) -> None:
                    "live": {"dyn_rows": r2, "static_rows": r1, "pairs": int(st["n_pairs"]),
                             "contacts": int(st["n_dyn_groups"]), "colors": int(st["n_colors"])},
                    "launch_shape": {"group_size": s.primal_group_size, "blocks_per_sm": s.blocks_per_sm,
-                                    "flag_sweep": bool(s.flag_sweep), "autotuned": tuned is not None},
+                                    "flag_sweep": bool(s.flag_sweep), "adaptive_lanes": bool(s.adaptive_lanes),
+                                    "autotuned": tuned is not None},
                    "scene_build_s": round(t_build, 2)},
         "roofline": {"bound": "hbm", "kernel": "k_solve_persistent", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -366,7 +367,8 @@ def run_gpu(args) -> None:
     }
     if tuned is not None:
         line["autotune_ms_per_frame"] = {
-            f"G{r['group_size']}x{r['blocks_per_sm']}{'-flags' if r['flag_sweep'] else ''}": round(r["ms_per_frame"], 3)
+            (f"G{r['group_size']}x{r['blocks_per_sm']}{'-flags' if r['flag_sweep'] else ''}"
+             f"{'-adapt' if r['adaptive_lanes'] else ''}"): round(r["ms_per_frame"], 3)
             for r in tuned["table"]}
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

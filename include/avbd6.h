@@ -94,6 +94,11 @@ typedef struct AvbdParams {
   int flag_sweep;      /* persistent solve: order the color passes by per-body
                           completion flags (each body waits only for its own
                           neighbours) instead of a grid barrier per color */
+  int adaptive_lanes;  /* barrier sweep: a color whose bodies, at twice the
+                          lanes per body, still fit in one round of the
+                          resident warps gets twice the lanes (repeatedly,
+                          up to 32); group_size is then the lane count of
+                          the large colors */
 } AvbdParams;
 
 typedef struct AvbdStats {

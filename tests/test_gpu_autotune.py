@@ -19,10 +19,11 @@ def test_autotune_restores_state_and_applies_best():
     after = s.state_dict()
     for k in ("x", "q", "v", "w"):
         np.testing.assert_array_equal(before[k], after[k])
-    assert len(res["table"]) == 12 and all(r["ms_per_frame"] > 0 for r in res["table"])
+    # 3 group sizes x 2 CTA counts x (barrier, barrier + adaptive lanes, flags)
+    assert len(res["table"]) == 18 and all(r["ms_per_frame"] > 0 for r in res["table"])
     best = res["best"]
-    assert (s.primal_group_size, s.blocks_per_sm, s.flag_sweep) == (best["group_size"], best["blocks_per_sm"],
-                                                                    best["flag_sweep"])
+    assert (s.primal_group_size, s.blocks_per_sm, s.flag_sweep, s.adaptive_lanes) == (
+        best["group_size"], best["blocks_per_sm"], best["flag_sweep"], best["adaptive_lanes"])
     assert best["ms_per_frame"] == min(r["ms_per_frame"] for r in res["table"])
     # the tuned solver still steps: same trajectory as an untuned twin loaded with the same state
     s.step()
@@ -31,6 +32,7 @@ def test_autotune_restores_state_and_applies_best():
     t.primal_group_size = best["group_size"]
     t.blocks_per_sm = best["blocks_per_sm"]
     t.flag_sweep = best["flag_sweep"]
+    t.adaptive_lanes = best["adaptive_lanes"]
     t.load_state_dict(before)
     t.step()
     np.testing.assert_allclose(s.state_dict()["x"], t.state_dict()["x"], atol=1e-6)
