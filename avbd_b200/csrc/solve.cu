@@ -715,11 +715,13 @@ __device__ __forceinline__ void prefetch_group_fixed(const Dev& d, int g, bool b
 
 // Flag-ordered sweep: all `total` passes over the colors without a grid
 // barrier.  The work is cut into chunks of W = 32/G bodies of one color of
-// one pass, numbered in (pass, color) order; warp w takes chunks w, w +
-// warps, w + 2 warps, ...  A body waits only for its own previous pass and
-// for its neighbours (lower color: this pass; higher color: the previous
-// pass), so every chunk depends only on lower-numbered chunks and the lowest
-// unfinished chunk can always run (all warps are resident).  Each body's
+// one pass, numbered in (pass, color) order; warp w starts on chunk w and
+// then takes the next undealt chunk from a counter, so chunks are dealt in
+// increasing order to whichever warp is free.  A body waits only for its own
+// previous pass and for its neighbours (lower color: this pass; higher
+// color: the previous pass), so every chunk depends only on lower-numbered
+// chunks, all of them already dealt, and the lowest unfinished chunk can
+// always run (all warps are resident).  Each body's
 // arithmetic and reduction order are those of primal_color, so the results
 // are bit-identical to the barrier sweep.
 template <int G, bool B>
@@ -741,7 +743,7 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
   }
   const int per_pass = __shfl_sync(FULL, incl, 31);
   const long long n_chunks = (long long)per_pass * total;
-  for (long long q = gtid >> 5; q < n_chunks; q += gsize >> 5) {
+  for (long long q = gtid >> 5; q < n_chunks;) {
     int it = (int)(q / per_pass), r = (int)(q - (long long)it * per_pass);
     int c = __ffs(__ballot_sync(FULL, incl > r)) - 1;
     int cntc = __shfl_sync(FULL, cnt, c);
@@ -814,6 +816,9 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
     __syncwarp();
     if (act && gl == 0) st_release(d.done + i, it + 1);
     if (pm.viol_slot >= 0) record_violation(d, pm.viol_slot, vmax, csum, ccnt);
+    int next = 0;
+    if (lane == 0) next = atomicAdd(&d.ctr->work_ctr[0], 1);  // zeroed at the substep start
+    q = (gsize >> 5) + (long long)__shfl_sync(FULL, next, 0);
   }
 }
 
