@@ -485,6 +485,9 @@ int avbd_cache_load_keys(AvbdCtx* c, int n, const unsigned long long* keys, cons
 int avbd_clear_errors(AvbdCtx* c, void* stream) {
   if (!c) return fail(AVBD_E_INVALID, "null ctx");
   cudaError_t e = cudaMemsetAsync(&c->d.ctr->err, 0, 2 * sizeof(int), (cudaStream_t)stream);
+  // a solve that stopped early may leave the coloring flags set
+  if (e == cudaSuccess && c->d.nb > 0)
+    e = cudaMemsetAsync(c->d.c_lost, 0, (size_t)c->d.nb * sizeof(int), (cudaStream_t)stream);
   return e == cudaSuccess ? AVBD_OK : fail(AVBD_E_CUDA, "clear errors", e);
 }
 

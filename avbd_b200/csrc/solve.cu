@@ -1288,6 +1288,13 @@ __device__ void ph_resolve_apply(const Dev& d, int* unc_out, int gtid, int gsize
 // thread's current body, and everything it waits for has published, so it
 // always advances.  Returns false (nothing done) when a thread would hold
 // more than 32 bodies; the caller then runs the round loop.
+//
+// It runs speculatively, before the gate has decided whether to recolor:
+// it reads only the contact graph and the priorities and writes color2 (-1
+// = uncolored) and st = c_lost, which must be zero on entry (the arena
+// starts zeroed; the persistent kernel clears it after every use, and so
+// does avbd_clear_errors after a launch that stopped early).  When the gate
+// keeps the old coloring, color2 is simply not used.
 #define DF_HP 8
 __device__ __forceinline__ int ld_relaxed(const int* p) {
   int v;
@@ -1371,8 +1378,8 @@ __device__ __noinline__ bool ph_color_dataflow(const Dev& d, int gtid, int gsize
         r = JP_ROUNDS;
       } else {
         c = first_fit((int)used);
-        d.color[cur] = c;
       }
+      d.color2[cur] = c < MAX_COLORS ? c : -1;
       asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(st + cur), "r"(1 + (r << 6) + c) : "memory");
       take_next();
       continue;
@@ -1403,7 +1410,8 @@ __device__ __forceinline__ int bucket_key(const Dev& d, int i, int c) {
   return 2 * c + (work > HEAVY_GROUPS ? 0 : 1);
 }
 
-__device__ void ph_bucket_count(const Dev& d) {
+// from_color2: the colors come from the speculative dataflow coloring.
+__device__ void ph_bucket_count(const Dev& d, bool from_color2 = false) {
   __shared__ int h[NKEY];
   int cs = (d.nb + NCH - 1) / NCH;
   for (int b = blockIdx.x; b < NCH; b += gridDim.x) {
@@ -1411,10 +1419,10 @@ __device__ void ph_bucket_count(const Dev& d) {
     __syncthreads();
     int s0 = b * cs, s1 = min(d.nb, s0 + cs);
     for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
-      int c = d.color[i];
-      if (c < 0) {  // stragglers take color 0 (kernels_6dof.py:3151-3165)
-        c = 0;
-        d.color[i] = 0;
+      int c = from_color2 ? d.color2[i] : d.color[i];
+      if (c < 0 || from_color2) {  // stragglers take color 0 (kernels_6dof.py:3151-3165)
+        c = max(c, 0);
+        d.color[i] = c;
       }
       atomicAdd(&h[bucket_key(d, i, c)], 1);
     }
@@ -1524,20 +1532,26 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
     d.ctr->mark_id[0] = PH_START;
     d.ctr->n_marks = 1;
   }
+  const bool jp = P.color_mode == 1;
+  // Jones-Plassmann: the dataflow coloring runs alongside the gate and the
+  // prelude, into color2, and is used only if the gate asks for new colors.
+  const bool spec = jp && (long long)d.nb <= 32LL * gsize;
   ph_gate(d, gtid, gsize);
   ph_prelude<BATCHED>(d, gtid, gsize);  // reads x/q = the initial pose; predict runs after
   ph_mlp_prelude(d, gtid, gsize);
+  if (spec) ph_color_dataflow(d, gtid, gsize);
   SYNC(PH_GATE_PRELUDE);
   if (recolor_needed(d)) {
-    bool jp = P.color_mode == 1;
-    ph_color_reset(d, gtid, gsize);
-    SYNC(PH_COLOR_RESET);
-    bool dataflow = jp && ph_color_dataflow(d, gtid, gsize);
-    if (dataflow) SYNC(PH_ROUND);
+    if (spec) {
+      if (gtid == 0) d.ctr->recolored = 1;
+    } else {
+      ph_color_reset(d, gtid, gsize);
+      SYNC(PH_COLOR_RESET);
+    }
     // Round r counts its uncolored bodies into round_unc[r & 1]; every block
     // reads it after the round's last barrier.  The other slot is cleared
     // during round r's second phase, when all blocks have read it.
-    int rounds = dataflow ? 0 : (jp ? JP_ROUNDS : MAX_COLORS);
+    int rounds = spec ? 0 : (jp ? JP_ROUNDS : MAX_COLORS);
     for (int r = 0; r < rounds; ++r) {
       int* unc_slot = &d.ctr->round_unc[r & 1];
       ph_round_edges(d, jp, gtid, gsize);
@@ -1553,7 +1567,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
       }
       if (*(volatile int*)unc_slot == 0) break;
     }
-    ph_bucket_count(d);
+    ph_bucket_count(d, spec);
     SYNC(PH_BUCKET);
     ph_bucket_scan(d);
     SYNC(PH_BUCKET);
@@ -1590,6 +1604,8 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
     SYNC(PH_DUAL);
   }
   ph_collect(d, gtid, gsize);
+  if (spec)
+    for (int i = gtid; i < d.nb; i += gsize) d.c_lost[i] = 0;  // the dataflow's flags, for the next launch
   SYNC(PH_COLLECT);
   if (gtid == 0) {
     d.ctr->epoch += 1u;
