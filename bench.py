@@ -243,6 +243,9 @@ def run_gpu(args) -> None:
         s.primal_group_size = args.group_size
     if args.blocks_per_sm:
         s.blocks_per_sm = args.blocks_per_sm
+    if args.sweep:
+        s.flag_sweep = args.sweep == "flags"
+        s.adaptive_lanes = args.sweep == "barrier-adaptive"
     t_build = time.perf_counter()
     scenes.pile(s, **size)
     s._flush()  # host scene build + arena upload, timed for the report
@@ -252,7 +255,7 @@ def run_gpu(args) -> None:
         s._enqueue_step()
     s._after_frame()
     tuned = None
-    if not (args.no_tune or args.group_size or args.blocks_per_sm):
+    if not (args.no_tune or args.group_size or args.blocks_per_sm or args.sweep):
         from avbd_b200.autotune import autotune
         tuned = autotune(s)  # launch shape for this scene; the scene state is restored
     for _ in range(args.warmup):
@@ -332,12 +335,15 @@ def run_gpu(args) -> None:
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = ab["solve"] / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
     # DRAM bytes of one solve launch from an ncu capture of this workload
-    # (dram__bytes_read.sum + dram__bytes_write.sum), committed with its command
+    # (dram__bytes_read.sum + dram__bytes_write.sum), committed with its
+    # command; the capture's pile settled fewer frames, so its bytes are
+    # scaled by the ratio of the two launches' algorithmic bytes
     traffic = None
     tf = os.path.join(ROOT, "profiles", "solve_traffic.json")
     if os.path.exists(tf) and not args.small:
         try:
-            traffic = json.load(open(tf)).get("bytes_per_launch")
+            cap = json.load(open(tf))
+            traffic = cap["bytes_per_launch"] * ab["solve"] / cap.get("algorithmic_bytes_per_launch", ab["solve"])
         except Exception:
             traffic = None
     line = {
@@ -511,6 +517,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--group-size", type=int, default=0, help="lanes per body (0 = autotuned)")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="solve CTAs per SM (0 = autotuned)")
+    ap.add_argument("--sweep", default="", choices=["", "barrier", "barrier-adaptive", "flags"],
+                    help="color-pass ordering (empty = autotuned)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start evaluation")
     ap.add_argument("--row-capacity", type=int, default=0, help="initial dynamic-row pool (0 = reference size)")
