@@ -33,7 +33,8 @@ class AvbdParams(C.Structure):
                 ("group_size", C.c_int), ("use_graph", C.c_int), ("persistent", C.c_int),
                 ("record_violation", C.c_int), ("mlp_warm_start", C.c_int), ("debug_skip_arrive", C.c_int),
                 ("blocks_per_sm", C.c_int), ("timing", C.c_int), ("log_new_contacts", C.c_int),
-                ("flag_sweep", C.c_int), ("adaptive_lanes", C.c_int)]
+                ("flag_sweep", C.c_int), ("bvh_rebuild_every", C.c_int),
+                ("adaptive_lanes", C.c_int)]
 
 
 class AvbdStats(C.Structure):

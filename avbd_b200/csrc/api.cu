@@ -108,12 +108,16 @@ struct AvbdCtx {
   int num_sms;
   int coll_grid;
   int solve_grid, solve_block, solve_variant;
-  cudaGraphExec_t exec[2];
-  cudaGraph_t graph[2];
-  bool graph_ok[2];
-  int graph_key[2][4];
-  int capture_err[2];
-  int part_kernels[2];
+  // parts: 0 = collision with an LBVH rebuild, 1 = solve, 2 = collision
+  // that refits the previous tree
+  cudaGraphExec_t exec[3];
+  cudaGraph_t graph[3];
+  bool graph_ok[3];
+  int graph_key[3][4];
+  int capture_err[3];
+  int part_kernels[3];
+  int bvh_age;        // substeps since the last LBVH rebuild (0: none yet)
+  int last_coll_part; // collision part of the last substep
   long long kernels_launched;
   long long substeps_done;
   float cur_dt;
@@ -228,8 +232,7 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
 
 int avbd_destroy(AvbdCtx* c) {
   if (!c) return AVBD_OK;
-  drop_graph(c, 0);
-  drop_graph(c, 1);
+  for (int part = 0; part < 3; ++part) drop_graph(c, part);
   for (int k = 0; k < 3; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   delete c;
@@ -309,8 +312,8 @@ int avbd_mark_color_dirty(AvbdCtx* c, void* stream) {
 static cudaError_t enqueue_part(AvbdCtx* c, int part, cudaStream_t st) {
   long long before = g_kernel_launches;
   cudaError_t e;
-  if (part == 0) {
-    launch_collision(c->d, c->P, c->dims, c->coll_grid, st);
+  if (part != 1) {
+    launch_collision(c->d, c->P, c->dims, c->coll_grid, st, part == 0);
     e = cudaGetLastError();
   } else {
     e = launch_solve(c->d, c->P, c->P.persistent, c->solve_grid, c->solve_block, st, c->solve_variant);
@@ -320,7 +323,7 @@ static cudaError_t enqueue_part(AvbdCtx* c, int part, cudaStream_t st) {
 }
 
 static void part_key(AvbdCtx* c, int part, int key[4]) {
-  if (part == 0) {
+  if (part != 1) {
     key[0] = c->P.self_collide; key[1] = c->coll_grid; key[2] = 0; key[3] = 0;
   } else {
     key[0] = c->P.persistent + 10 * c->solve_variant; key[1] = c->solve_grid;
@@ -380,8 +383,16 @@ static cudaError_t run_part(AvbdCtx* c, int part, cudaStream_t st) {
 static int run_substep(AvbdCtx* c, cudaStream_t st) {
   if (c->d.nb == 0) return AVBD_OK;
   if (c->substeps_done > 0 && c->substeps_done % 8192 == 0) launch_hash_scrub(c->d, st);
+  // The pair list does not depend on the tree (pairs come out sorted by
+  // body), so between rebuilds the LBVH is only refit to the new boxes.
+  bool collide = c->P.self_collide && c->d.nb >= 2;
+  int every = c->P.bvh_rebuild_every > 1 ? c->P.bvh_rebuild_every : 1;
+  bool rebuild = !collide || c->bvh_age == 0 || c->bvh_age >= every;
+  int part = rebuild ? 0 : 2;
+  c->bvh_age = !collide ? 0 : (rebuild ? 1 : c->bvh_age + 1);
+  c->last_coll_part = part;
   cudaEventRecord(c->ev[0], st);
-  cudaError_t e = run_part(c, 0, st);
+  cudaError_t e = run_part(c, part, st);
   if (e != cudaSuccess) return fail(AVBD_E_CUDA, "collision launch", e);
   cudaEventRecord(c->ev[1], st);
   e = run_part(c, 1, st);
@@ -449,8 +460,8 @@ int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {
   out->max_dg = h.max_dg;
   out->n_viol = h.n_viol;
   out->epoch = h.epoch;
-  out->graph_state = (c->graph_ok[0] ? 1 : 0) | (c->graph_ok[1] ? 2 : 0);
-  out->capture_err = c->capture_err[0] * 1000 + c->capture_err[1];
+  out->graph_state = (c->graph_ok[c->last_coll_part] ? 1 : 0) | (c->graph_ok[1] ? 2 : 0);
+  out->capture_err = c->capture_err[c->last_coll_part] * 1000 + c->capture_err[1];
   out->kernels_launched = c->kernels_launched;
   out->n_new_logged = h.n_new_logged;
   out->n_mlp_applied = h.n_mlp_applied;

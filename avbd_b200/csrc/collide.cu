@@ -347,6 +347,18 @@ __global__ void k_lbvh_build(const __grid_constant__ Dev d) {
   if (blockIdx.x == 0 && threadIdx.x == 0) d.node_parent[0] = -1;
 }
 
+// Between rebuilds: the tree keeps its topology and leaf order; leaves take
+// the bodies' new boxes and the refit below recomputes the internal ones.
+__global__ void k_lbvh_leaves(const __grid_constant__ Dev d) {
+  int n = d.nb;
+  GSTRIDE(i, n - 1) d.node_flag[i] = 0;
+  GSTRIDE(k, n) {
+    int b = d.order[k];
+    d.node_lo[n - 1 + k] = d.aabb_lo[b];
+    d.node_hi[n - 1 + k] = d.aabb_hi[b];
+  }
+}
+
 __global__ void k_lbvh_refit(const __grid_constant__ Dev d) {
   int n = d.nb;
   GSTRIDE(k, n) {
@@ -943,7 +955,7 @@ __global__ void k_dg_clear(const __grid_constant__ Dev d) {
 // ---------------------------------------------------------------------------
 // Host-side launch sequence of the collision pipeline.
 // ---------------------------------------------------------------------------
-void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int grid, cudaStream_t st) {
+void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int grid, cudaStream_t st, bool rebuild) {
   k_begin_substep<<<grid, 256, 0, st>>>(d);
   bool collide = P.self_collide && d.nb >= 2;
   if (!collide) {
@@ -952,9 +964,13 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
     return;
   }
   k_aabb<<<grid, 256, 0, st>>>(d);
-  k_morton<<<grid, 256, 0, st>>>(d);
-  radix_sort_launch(d, st);
-  k_lbvh_build<<<grid, 256, 0, st>>>(d);
+  if (rebuild) {
+    k_morton<<<grid, 256, 0, st>>>(d);
+    radix_sort_launch(d, st);
+    k_lbvh_build<<<grid, 256, 0, st>>>(d);
+  } else {
+    k_lbvh_leaves<<<grid, 256, 0, st>>>(d);  // same topology, new leaf boxes
+  }
   k_lbvh_refit<<<grid, 256, 0, st>>>(d);
   k_bp_count<<<grid, 128, 0, st>>>(d);
   scan_launch(d, d.up_cnt, d.pair_start, d.nb, nullptr, nullptr, st);
@@ -968,7 +984,7 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
   k_dg_zero<<<grid, 256, 0, st>>>(d);
   k_dg_fill<<<grid, 256, 0, st>>>(d);
   k_dg_sort<<<grid, 128, 0, st>>>(d);
-  g_kernel_launches += 13;  // the direct launches above (scans and sort count themselves)
+  g_kernel_launches += rebuild ? 12 : 11;  // the direct launches above (scans and sort count themselves)
 }
 
 }  // namespace avbd

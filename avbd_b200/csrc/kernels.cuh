@@ -11,7 +11,7 @@ extern thread_local long long g_kernel_launches;
 void scan_launch(const Dev& d, const int* in, int* out, int n_cap, const int* n_dev, int* total_out,
                  cudaStream_t st);
 void radix_sort_launch(Dev& d, cudaStream_t st);
-void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int grid, cudaStream_t st);
+void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int grid, cudaStream_t st, bool rebuild = true);
 
 // Solve: coloring + predict + prelude + iterations + cache refresh.
 // persistent = one cooperative launch; otherwise one launch per phase.

@@ -302,6 +302,8 @@ class Solver6DOF:
         # flags instead of one grid barrier per color (same results)
         self.flag_sweep = False
         self.adaptive_lanes = False  # more lanes per body for small colors (barrier sweep)
+        # LBVH rebuilt every this many substeps, refit in between (same pairs)
+        self.bvh_rebuild_every = 8
         # initial dynamic-row pool (None: the reference's 192 rows per body)
         self.dyn_row_capacity = None
         self._anchor_keys = False  # cache_key_mode "anchor_5mm"
@@ -684,6 +686,7 @@ class Solver6DOF:
         p.log_new_contacts = int(self._log_new)
         p.flag_sweep = int(bool(self.flag_sweep))
         p.adaptive_lanes = int(bool(self.adaptive_lanes))
+        p.bvh_rebuild_every = max(1, int(self.bvh_rebuild_every))
         if self._scene_tab:  # the device loops cover the largest scene settings
             p.substeps = max(sc for sc, _ in self._scene_tab)
             p.iterations = max(it for _, it in self._scene_tab)

@@ -94,6 +94,9 @@ typedef struct AvbdParams {
   int flag_sweep;      /* persistent solve: order the color passes by per-body
                           completion flags (each body waits only for its own
                           neighbours) instead of a grid barrier per color */
+  int bvh_rebuild_every; /* collision: rebuild the LBVH every this many
+                          substeps and refit it in between (the pair list
+                          is the same either way); 0 or 1 = every substep */
   int adaptive_lanes;  /* barrier sweep: a color whose bodies, at twice the
                           lanes per body, still fit in one round of the
                           resident warps gets twice the lanes (repeatedly,
