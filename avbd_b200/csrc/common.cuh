@@ -28,6 +28,18 @@ __host__ __device__ inline int meta_cidx(int m) { return (m >> 4) & 3; }
 __host__ __device__ inline int make_meta(int kind, int three, int hard, int cidx) {
   return kind | (three ? 4 : 0) | (hard ? 8 : 0) | (cidx << 4);
 }
+// Implicit floor corners (bit 9): the 8 corner groups of one floor block
+// (solver_6dof.py:474-541) store no geometry.  The corner offset is the
+// body's half extents with the signs of corner index c = bits 6-8 (x: bit 2,
+// y: bit 1, z: bit 0; set = +, the reference's sx, sy, sz loop order), and
+// g_mat.w, the fracture threshold of other groups (never reached by floor
+// rows), holds the floor height.
+#define META_IMPLICIT 512
+__host__ __device__ inline bool meta_implicit(int m) { return (m & META_IMPLICIT) != 0; }
+__device__ __forceinline__ float4 implicit_corner(float4 he, int meta, float floor_y) {
+  int c = (meta >> 6) & 7;
+  return make_float4((c & 4) ? he.x : -he.x, (c & 2) ? he.y : -he.y, (c & 1) ? he.z : -he.z, floor_y);
+}
 // g_flags bit layout: bits 0-2 row active, bit 3 normal row was_static,
 // bits 4/5 the friction rows' own was_static (carried to the cache), bit 6:
 // body_b owns the group (runs its dual update; else body_a), bit 7: a new

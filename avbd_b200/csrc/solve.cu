@@ -329,7 +329,13 @@ __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3
   float sg = 1.0f;
   bool own = true;
   if (kind == KIND_FLOOR) {
-    float4 oa = d.g_offa[g];
+    float4 oa;
+    if (meta_implicit(meta)) {
+      oa = implicit_corner(d.he[i], meta, mat.w);
+      mat.w = FINF;  // no fracture on floor rows
+    } else {
+      oa = d.g_offa[g];
+    }
     rs = qrot(qi, xyz(oa));
     C[0] = (xi.y + rs.y) - oa.w;
     C[1] = xi.x + rs.x;  // dot((1,0,0), x + R off)
@@ -831,7 +837,7 @@ __device__ __forceinline__ GroupC group_values(const Dev& d, int g, int meta, co
   GroupC r;
   int kind = meta_kind(meta);
   int2 bd = d.g_body[g];
-  float4 oa = d.g_offa[g];
+  float4 oa = meta_implicit(meta) ? implicit_corner(d.he[bd.x], meta, d.g_mat[g].w) : d.g_offa[g];
   float4 xa = X[bd.x], qa = Q[bd.x];
   V3 pa = xyz(xa) + qrot(qa, xyz(oa));
   if (kind == KIND_FLOOR) {
@@ -1002,6 +1008,7 @@ __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
     int kind = meta_kind(meta);
     bool three = (meta & 4) != 0, hard = (meta & 8) != 0;
     float4 lam = d.g_lam[g], pen = d.g_pen[g], ac0 = d.g_ac0[g], mat = d.g_mat[g];
+    if (meta_implicit(meta)) mat.w = FINF;  // w holds the floor height
     GroupC cv = group_values(d, g, meta, d.x, d.q);
     float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z}, ac[3] = {ac0.x, ac0.y, ac0.z};
     if (fl & FL_LRN) learned_check(d, kind, hard, cv.c, ac, lm, pn, fl);

@@ -31,6 +31,7 @@ PIN_6DOF = 2
 BOX_BOX_CONTACT_6DOF = 3
 
 KIND_FLOOR, KIND_PIN, KIND_BOX = 0, 1, 2
+META_IMPLICIT = 512  # implicit floor corner (corner index in meta bits 6-8; csrc/common.cuh)
 MAX_COLORS = 32
 _INF = math.inf
 
@@ -540,13 +541,24 @@ class Solver6DOF:
             r0 = np.array([f[6] for f in fb], np.int64)
             per = np.array([f[7] for f in fb], np.int64)
             body[:nf, 0] = np.repeat(bb, 8)
-            offa[:nf, :3] = (he[:, None, :] * _CORNER_SIGNS[None, :, :]).reshape(-1, 3).astype(np.float32)
-            offa[:nf, 3] = np.repeat(fy, 8)
             row0[:nf] = (r0[:, None] + np.arange(8)[None, :] * per[:, None]).reshape(-1)
             three[:nf] = np.repeat(per == 3, 8)
             hard = np.repeat(~(st < _INF), 8)
             meta[:nf] = KIND_FLOOR | np.where(three[:nf], 4, 0) | np.where(hard, 8, 0)
             mat[:nf] = np.repeat(np.stack([mu, mus, st, np.full_like(st, _INF)], 1), 8, axis=0)
+            # Implicit corners: a block whose half extents are its body's
+            # stores no offsets; the kernels rebuild them from the body's half
+            # extents and the corner index (meta bits 6-8), and the floor
+            # height sits in mat.w.  Other blocks keep explicit offsets.
+            body_he = np.asarray(self._half_extents, np.float32).reshape(-1, 3)[bb]
+            imp = np.all(he.astype(np.float32) == body_he, axis=1)
+            imp8 = np.repeat(imp, 8)
+            corner = np.tile(np.arange(8), len(fb))
+            meta[:nf] |= np.where(imp8, META_IMPLICIT | (corner << 6), 0).astype(np.int32)
+            explicit = (he[:, None, :] * _CORNER_SIGNS[None, :, :]).reshape(-1, 3).astype(np.float32)
+            offa[:nf, :3] = np.where(imp8[:, None], 0.0, explicit)
+            offa[:nf, 3] = np.where(imp8, 0.0, np.repeat(fy, 8))
+            mat[:nf, 3] = np.where(imp8, np.repeat(fy, 8), mat[:nf, 3])
         for j, (kind, b, r0_, th, off, extra, mu_, mus_, stiff, frac) in enumerate(self._groups):
             k = nf + j
             body[k, 0] = b
