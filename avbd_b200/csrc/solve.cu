@@ -778,9 +778,16 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
       int e0 = d.dg_start[i], nd = d.dg_start[i + 1] - e0;
       // No L1 prefetch here: the lines of a chunk's ~10 SoA arrays do not
       // survive in L1 until they are read (measured: 0.6 % faster without).
-      for (int kk = gl; kk < ns + nd; kk += G) {
-        int g = kk < ns ? s0 + kk : d.dg_idx[e0 + (kk - ns)];
+      // The next group's index is loaded before this group is evaluated, so
+      // its round trip overlaps the evaluation (3.5 % faster; also loading
+      // the next group's body pair that early measured slower).
+      const int nt = ns + nd;
+      int g = gl < ns ? s0 + gl : (gl < nt ? d.dg_idx[e0 + (gl - ns)] : 0);
+      for (int kk = gl; kk < nt; kk += G) {
+        int kn = kk + G;
+        int gn = kn < ns ? s0 + kn : (kn < nt ? d.dg_idx[e0 + (kn - ns)] : 0);
         vmax = fmaxf(vmax, accumulate_group<true>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt, it, c));
+        g = gn;
       }
     }
     if (G > 1) {
