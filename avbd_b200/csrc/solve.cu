@@ -758,6 +758,17 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
       act = act && on;
       solve = act && (pm.it < its || post_stab);
     }
+    // The incidence ranges and this lane's first group do not change during
+    // the passes: their loads go out before the wait for the body's previous
+    // pass, not after it.
+    int s0 = 0, ns = 0, e0 = 0, nd = 0, g = 0;
+    if (act) {
+      s0 = d.sg_start[i];
+      ns = d.sg_start[i + 1] - s0;
+      e0 = d.dg_start[i];
+      nd = d.dg_start[i + 1] - e0;
+      g = gl < ns ? s0 + gl : (gl < ns + nd ? d.dg_idx[e0 + (gl - ns)] : 0);
+    }
     float4 xi4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), qi = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
     if (act) {
       wait_done(d, i, it);  // its own previous pass (possibly on another SM)
@@ -774,15 +785,13 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
     int ccnt = 0;
     if (act) {
       V3 xi = xyz(xi4);
-      int s0 = d.sg_start[i], ns = d.sg_start[i + 1] - s0;
-      int e0 = d.dg_start[i], nd = d.dg_start[i + 1] - e0;
       // No L1 prefetch here: the lines of a chunk's ~10 SoA arrays do not
       // survive in L1 until they are read (measured: 0.6 % faster without).
       // The next group's index is loaded before this group is evaluated, so
-      // its round trip overlaps the evaluation (3.5 % faster; also loading
-      // the next group's body pair that early measured slower).
+      // its round trip overlaps the evaluation (0.5-3.5 % faster on different
+      // boxes; also loading the next group's body pair that early measured
+      // slower).
       const int nt = ns + nd;
-      int g = gl < ns ? s0 + gl : (gl < nt ? d.dg_idx[e0 + (gl - ns)] : 0);
       for (int kk = gl; kk < nt; kk += G) {
         int kn = kk + G;
         int gn = kn < ns ? s0 + kn : (kn < nt ? d.dg_idx[e0 + (kn - ns)] : 0);
