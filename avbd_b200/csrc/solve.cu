@@ -1409,15 +1409,19 @@ __device__ __noinline__ bool ph_color_dataflow(const Dev& d, int gtid, int gsize
   return true;
 }
 
-// Bucketing of bodies by color.  Within a color, bodies with many incident
-// groups come first (the longest jobs start in the first wave of a pass),
-// then by body index; deterministic.  Key = 2 * color + (light ? 1 : 0).
+// Bucketing of bodies by color.  Within a color, bodies come in four work
+// buckets, heaviest first: more than 24, 17-24, 9-16 and at most 8 incident
+// groups, i.e. by the lane rounds a body takes at 8 lanes.  The longest jobs
+// start in the first wave of a pass, and a 4-body chunk mostly holds bodies
+// with the same number of rounds, so few lanes idle.  Then by body index;
+// deterministic.  Key = 4 * color + bucket.
 #define NCH 64
-#define NKEY (2 * MAX_COLORS)
-#define HEAVY_GROUPS 16
+#define NBK 4
+#define NKEY (NBK * MAX_COLORS)
+#define BUCKET_WARPS 8  // ph_bucket_place runs with 256-thread blocks (launch_solve checks)
 __device__ __forceinline__ int bucket_key(const Dev& d, int i, int c) {
   int work = (d.sg_start[i + 1] - d.sg_start[i]) + (d.dg_start[i + 1] - d.dg_start[i]);
-  return 2 * c + (work > HEAVY_GROUPS ? 0 : 1);
+  return NBK * c + (work > 24 ? 0 : work > 16 ? 1 : work > 8 ? 2 : 3);
 }
 
 // from_color2: the colors come from the speculative dataflow coloring.
@@ -1462,10 +1466,10 @@ __device__ void ph_bucket_scan(const Dev& d) {
     for (int u = 0; u < NKEY; ++u) {
       kstart[u] = acc;
       acc += tot[u];
-      if (tot[u] > 0) mx = u >> 1;
+      if (tot[u] > 0) mx = u / NBK;
     }
     kstart[NKEY] = acc;
-    for (int c = 0; c <= MAX_COLORS; ++c) d.color_starts[c] = kstart[2 * c < NKEY ? 2 * c : NKEY];
+    for (int c = 0; c <= MAX_COLORS; ++c) d.color_starts[c] = kstart[NBK * c < NKEY ? NBK * c : NKEY];
     d.ctr->n_colors = max(1, min(mx + 1, MAX_COLORS));
     d.ctr->color_dirty = 0;
   }
@@ -1477,7 +1481,7 @@ __device__ void ph_bucket_scan(const Dev& d) {
 
 __device__ void ph_bucket_place(const Dev& d) {
   __shared__ int run[NKEY];
-  __shared__ int wc[32][NKEY];
+  __shared__ int wc[BUCKET_WARPS][NKEY];
   int cs = (d.nb + NCH - 1) / NCH;
   int w = threadIdx.x >> 5, l = lane_id();
   int nw = blockDim.x >> 5;
@@ -1485,7 +1489,7 @@ __device__ void ph_bucket_place(const Dev& d) {
     if (threadIdx.x < NKEY) run[threadIdx.x] = d.c_hist[b * NKEY + threadIdx.x];
     int s0 = b * cs, s1 = min(d.nb, s0 + cs);
     for (int base = s0; base < s1; base += blockDim.x) {
-      for (int k = threadIdx.x; k < 32 * NKEY; k += blockDim.x) (&wc[0][0])[k] = 0;
+      for (int k = threadIdx.x; k < BUCKET_WARPS * NKEY; k += blockDim.x) (&wc[0][0])[k] = 0;
       __syncthreads();
       int i = base + threadIdx.x;
       bool valid = i < s1;
@@ -1727,6 +1731,8 @@ int solve_occupancy(int block, int variant) {
 
 cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st,
                          int variant) {
+  // the bucket phases size their per-warp tables for this block size
+  if (block != SOLVE_BLOCK) return cudaErrorInvalidConfiguration;
   // dynamic shared memory: the learned warm start's weights, when present
   size_t mlp_smem = d.mlp_w != nullptr ? sizeof(float) * AVBD_MLP_FLOATS : 0;
   if (persistent) {
