@@ -44,7 +44,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(C_HIST, 4, 64 * 128) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
   X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
   X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS) X(DONE, 4, N)              \
-  X(G_KEY, 8, KEYS ? G : 0)
+  X(G_KEY, 8, KEYS ? G : 0) X(NODE_REC, 64, N)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,
@@ -195,6 +195,7 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.order = PTR(int*, ORDER); d.order2 = PTR(int*, ORDER2);
   d.node_lo = PTR(float4*, NODE_LO); d.node_hi = PTR(float4*, NODE_HI); d.node_left = PTR(int*, NODE_LEFT);
   d.node_right = PTR(int*, NODE_RIGHT); d.node_parent = PTR(int*, NODE_PARENT); d.node_flag = PTR(int*, NODE_FLAG);
+  d.node_rec = PTR(float4*, NODE_REC);
   d.bounds = PTR(float*, BOUNDS);
   d.nbr_cnt = d.nbr_start = d.nbr_idx = d.nbr_pair = nullptr;
   d.up_cnt = PTR(int*, UP_CNT); d.pair_start = PTR(int*, PAIR_START); d.bp_tmp = PTR(int*, BP_TMP);

@@ -381,6 +381,23 @@ __global__ void k_lbvh_refit(const __grid_constant__ Dev d) {
   }
 }
 
+// Traversal copy of the tree: internal node p's record is four float4s,
+// (left lo, left index), (left hi, right index), (right lo), (right hi), so
+// one visit reads 64 contiguous bytes and needs no dependent load for its
+// children's boxes.  Written after every refit.
+__global__ void k_lbvh_pack(const __grid_constant__ Dev d) {
+  int n = d.nb;
+  GSTRIDE(p, n - 1) {
+    int l = d.node_left[p], r = d.node_right[p];
+    float4 a = d.node_lo[l], b = d.node_hi[l], c = d.node_lo[r], e = d.node_hi[r];
+    float4* rec = d.node_rec + 4 * (size_t)p;
+    rec[0] = make_float4(a.x, a.y, a.z, __int_as_float(l));
+    rec[1] = make_float4(b.x, b.y, b.z, __int_as_float(r));
+    rec[2] = make_float4(c.x, c.y, c.z, 0.0f);
+    rec[3] = make_float4(e.x, e.y, e.z, 0.0f);
+  }
+}
+
 __device__ __forceinline__ bool overlap(float4 alo, float4 ahi, float4 blo, float4 bhi) {
   return alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z && blo.z <= ahi.z;
 }
@@ -409,9 +426,11 @@ __device__ __forceinline__ void bvh_query_upper(const Dev& d, int i, F fn) {
   int sp = 0;
   int node = 0;
   while (true) {
-    int l = d.node_left[node], r = d.node_right[node];
-    bool ol = overlap(lo, hi, d.node_lo[l], d.node_hi[l]);
-    bool orr = overlap(lo, hi, d.node_lo[r], d.node_hi[r]);
+    const float4* rec = d.node_rec + 4 * (size_t)node;
+    float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
+    int l = __float_as_int(r0.w), r = __float_as_int(r1.w);
+    bool ol = overlap(lo, hi, r0, r1);
+    bool orr = overlap(lo, hi, r2, r3);
     if (ol && l >= n - 1) {
       leaf(l);
       ol = false;
@@ -972,6 +991,7 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
     k_lbvh_leaves<<<grid, 256, 0, st>>>(d);  // same topology, new leaf boxes
   }
   k_lbvh_refit<<<grid, 256, 0, st>>>(d);
+  k_lbvh_pack<<<grid, 256, 0, st>>>(d);
   k_bp_count<<<grid, 128, 0, st>>>(d);
   scan_launch(d, d.up_cnt, d.pair_start, d.nb, nullptr, nullptr, st);
   k_bp_fill<<<grid, 128, 0, st>>>(d);
@@ -984,7 +1004,7 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
   k_dg_zero<<<grid, 256, 0, st>>>(d);
   k_dg_fill<<<grid, 256, 0, st>>>(d);
   k_dg_sort<<<grid, 128, 0, st>>>(d);
-  g_kernel_launches += rebuild ? 12 : 11;  // the direct launches above (scans and sort count themselves)
+  g_kernel_launches += rebuild ? 13 : 12;  // the direct launches above (scans and sort count themselves)
 }
 
 }  // namespace avbd
