@@ -939,9 +939,13 @@ __global__ void k_dg_fill(const __grid_constant__ Dev d) {
     int g0 = d.n_sg + d.pair_gstart[p];
     int pa = d.dg_start[ab.x] + atomicAdd(&d.dg_cnt[ab.x], kept);
     int pb = d.dg_start[ab.y] + atomicAdd(&d.dg_cnt[ab.y], kept);
+    // the groups' bodies are (ref, inc) (k_emit); ab.x is the first when it is the reference
+    int a_second = ((d.pair_info[p] >> 9) & 1) ? 0 : 1;
     for (int c = 0; c < kept; ++c) {
       d.dg_idx[pa + c] = g0 + c;
       d.dg_idx[pb + c] = g0 + c;
+      d.dg_other[pa + c] = 2 * ab.y + a_second;
+      d.dg_other[pb + c] = 2 * ab.x + (1 - a_second);
     }
   }
 }
@@ -954,13 +958,15 @@ __global__ void k_dg_sort(const __grid_constant__ Dev d) {
   GSTRIDE(i, d.nb) {
     int s = d.dg_start[i], e = d.dg_start[i + 1];
     for (int a = s + 1; a < e; ++a) {
-      int v = d.dg_idx[a];
+      int v = d.dg_idx[a], w = d.dg_other[a];
       int b = a - 1;
       while (b >= s && d.dg_idx[b] > v) {
         d.dg_idx[b + 1] = d.dg_idx[b];
+        d.dg_other[b + 1] = d.dg_other[b];
         --b;
       }
       d.dg_idx[b + 1] = v;
+      d.dg_other[b + 1] = w;
     }
     if (e - s > 0) atomicMax(&d.ctr->max_dg, e - s);
   }

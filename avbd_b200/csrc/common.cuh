@@ -180,6 +180,7 @@ struct Dev {
   int *color, *color2, *color_starts, *color_bodies;
   int *sg_start;
   int *dg_start, *dg_cnt, *dg_idx;
+  int* dg_other;  // beside dg_idx: 2 * other body + (this body is the group's second body)
   // groups
   int2* g_body;
   int *g_meta, *g_row0, *g_flags;

@@ -302,22 +302,37 @@ __device__ __forceinline__ void learned_check(const Dev& d, int kind, bool hard,
 // one needs -- pass it+1 when it owns the group (lower color, already updated
 // in this pass), pass it otherwise -- and read everything another SM may
 // have written in this substep through L2 (__ldcg), never through L1.
+//
+// oe: for a box-box group, its incidence entry of body i (dg_other: 2 * the
+// other body + whether i is the group's second body), so the other body is
+// known without reading the group's body pair; -1 reads the pair.
 template <bool F>
 __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3 xi, float4 qi, bool post, bool dual,
-                                                  Acc& s, float& csum, int& ccnt, int it = 0, int ci = 0) {
+                                                  Acc& s, float& csum, int& ccnt, int it = 0, int ci = 0,
+                                                  int oe = -1) {
   int meta = d.g_meta[g];
   int fl = ldm<F>(d.g_flags + g);
   int kind = meta_kind(meta);
   bool three = (meta & 4) != 0, hard = (meta & 8) != 0;
   int nr = three ? 3 : 1;
+  int o = -1;
+  bool side_b = false;
+  if (kind == KIND_BOX) {
+    if (oe >= 0) {
+      o = oe >> 1;
+      side_b = (oe & 1) != 0;
+    } else {
+      int2 bd = d.g_body[g];
+      side_b = bd.x != i;
+      o = side_b ? bd.x : bd.y;
+    }
+  }
   if (F && kind == KIND_BOX) {
-    int2 bd = d.g_body[g];
-    int o = bd.x == i ? bd.y : bd.x;
     // A neighbour of the same color (a coloring that kept a conflict) runs
     // concurrently, as in the barrier sweep; waiting there could deadlock.
     if (d.color[o] != ci) {
       bool own_b = (fl & FL_OWNB) != 0;  // set before the passes; stable during them
-      bool i_owns = own_b == (bd.y == i);
+      bool i_owns = own_b == side_b;
       wait_done(d, o, i_owns ? it : it + 1);
       fl = ldm<F>(d.g_flags + g);  // after the owner's dual update of this pass
     }
@@ -348,10 +363,8 @@ __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3
     C[1] = p.y - an.y;
     C[2] = p.z - an.z;
   } else {
-    int2 bd = d.g_body[g];
-    bool side_a = bd.x == i;
+    bool side_a = !side_b;
     own = ((fl & FL_OWNB) != 0) == !side_a;
-    int o = side_a ? bd.y : bd.x;
     float4 xo4 = ldm<F>(d.x + o), qo = ldm<F>(d.q + o);
     float4 oa = d.g_offa[g], ob = d.g_offb[g];
     V3 n = xyz(d.g_n[g]);
@@ -761,13 +774,14 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
     // The incidence ranges and this lane's first group do not change during
     // the passes: their loads go out before the wait for the body's previous
     // pass, not after it.
-    int s0 = 0, ns = 0, e0 = 0, nd = 0, g = 0;
+    int s0 = 0, ns = 0, e0 = 0, nd = 0, g = 0, oe = -1;
     if (act) {
       s0 = d.sg_start[i];
       ns = d.sg_start[i + 1] - s0;
       e0 = d.dg_start[i];
       nd = d.dg_start[i + 1] - e0;
       g = gl < ns ? s0 + gl : (gl < ns + nd ? d.dg_idx[e0 + (gl - ns)] : 0);
+      oe = gl >= ns && gl < ns + nd ? d.dg_other[e0 + (gl - ns)] : -1;
     }
     float4 xi4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), qi = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
     if (act) {
@@ -795,8 +809,10 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
       for (int kk = gl; kk < nt; kk += G) {
         int kn = kk + G;
         int gn = kn < ns ? s0 + kn : (kn < nt ? d.dg_idx[e0 + (kn - ns)] : 0);
-        vmax = fmaxf(vmax, accumulate_group<true>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt, it, c));
+        int oen = kn >= ns && kn < nt ? d.dg_other[e0 + (kn - ns)] : -1;
+        vmax = fmaxf(vmax, accumulate_group<true>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt, it, c, oe));
         g = gn;
+        oe = oen;
       }
     }
     if (G > 1) {
