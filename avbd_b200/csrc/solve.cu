@@ -649,7 +649,8 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
       }
       for (int k = lane; k < ns + nd; k += G) {
         int g = k < ns ? s0 + k : d.dg_idx[e0 + (k - ns)];
-        vmax = fmaxf(vmax, accumulate_group<false>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt));
+        int oe = k < ns ? -1 : d.dg_other[e0 + (k - ns)];
+        vmax = fmaxf(vmax, accumulate_group<false>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt, 0, 0, oe));
       }
     }
     if (G > 1) {
@@ -1363,8 +1364,7 @@ __device__ __noinline__ bool ph_color_dataflow(const Dev& d, int gtid, int gsize
     for (int j = 0; j < DF_HP; ++j) hp[j] = -1;
     pending = 0;
     for (; kp < ke && pending < DF_HP; ++kp) {
-      int2 bd = d.g_body[d.dg_idx[kp]];
-      int o = bd.x == cur ? bd.y : bd.x;
+      int o = d.dg_other[kp] >> 1;
       if (o == last) continue;
       last = o;
       float po = d.prio[o];
