@@ -757,8 +757,7 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
     int cntc = __shfl_sync(FULL, cnt, c);
     int k = (r - __shfl_sync(FULL, incl - ch, c)) * W + slot;
     bool valid = k < cntc;
-    const int cstc = __shfl_sync(FULL, cst, c);  // every lane: the shuffle names the whole warp
-    int4 rec = valid ? d.chunk_rec[cstc + k] : make_int4(0, 0, 0, 0);
+    int4 rec = valid ? d.chunk_rec[__shfl_sync(FULL, cst, c) + k] : make_int4(0, 0, 0, 0);
     int i = rec.x;
     PassMode pm = pass_mode(P, it);
     float dt = P.dt;
