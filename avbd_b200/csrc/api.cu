@@ -44,7 +44,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(C_HIST, 4, 64 * 128) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
   X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
   X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS) X(DONE, 4, N)              \
-  X(G_KEY, 8, KEYS ? G : 0) X(NODE_REC, 64, N) X(DG_OTHER, 4, 2 * DG) X(CHUNK_REC, 16, N)
+  X(G_KEY, 8, KEYS ? G : 0) X(NODE_REC, 64, N) X(DG_OTHER, 4, 2 * DG)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,
@@ -187,7 +187,6 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.color_bodies = PTR(int*, COLOR_BODIES); d.sg_start = PTR(int*, SG_START); d.dg_start = PTR(int*, DG_START);
   d.dg_cnt = PTR(int*, DG_CNT); d.dg_idx = PTR(int*, DG_IDX);
   d.dg_other = PTR(int*, DG_OTHER);
-  d.chunk_rec = PTR(int4*, CHUNK_REC);
   d.g_body = PTR(int2*, G_BODY); d.g_meta = PTR(int*, G_META); d.g_row0 = PTR(int*, G_ROW0);
   d.g_flags = PTR(int*, G_FLAGS); d.g_offa = PTR(float4*, G_OFFA); d.g_offb = PTR(float4*, G_OFFB);
   d.g_n = PTR(float4*, G_N); d.g_mat = PTR(float4*, G_MAT); d.g_lam = PTR(float4*, G_LAM);

@@ -181,9 +181,6 @@ struct Dev {
   int *sg_start;
   int *dg_start, *dg_cnt, *dg_idx;
   int* dg_other;  // beside dg_idx: 2 * other body + (this body is the group's second body)
-  // per position of color_bodies: (body, first static group, first dynamic
-  // incidence, counts) -- see chunk_rec_of in solve.cu
-  int4* chunk_rec;
   // groups
   int2* g_body;
   int *g_meta, *g_row0, *g_flags;

@@ -740,8 +740,7 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
   const int post_stab = P.post_stab;
   const int slot_now = B ? d.ctr->slot : 0;
   // chunks per color (colors <= 32: one lane each), inclusive prefix
-  int cst = lane < nc ? d.color_starts[lane] : 0;
-  int cnt = lane < nc ? d.color_starts[lane + 1] - cst : 0;
+  int cnt = lane < nc ? d.color_starts[lane + 1] - d.color_starts[lane] : 0;
   int ch = (cnt + W - 1) / W;
   int incl = ch;
 #pragma unroll
@@ -757,11 +756,10 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
     int cntc = __shfl_sync(FULL, cnt, c);
     int k = (r - __shfl_sync(FULL, incl - ch, c)) * W + slot;
     bool valid = k < cntc;
-    int4 rec = valid ? d.chunk_rec[__shfl_sync(FULL, cst, c) + k] : make_int4(0, 0, 0, 0);
-    int i = rec.x;
+    int i = valid ? d.color_bodies[d.color_starts[c] + k] : 0;
     PassMode pm = pass_mode(P, it);
     float dt = P.dt;
-    bool act = valid && (rec.w == -1 ? d.x0[i].w > 0.0f : rec.w >= 0);  // mass > 0 (constant)
+    bool act = valid && d.x0[i].w > 0.0f;  // mass is constant; x0 was written before the passes
     bool solve = act;
     if (B) {
       float4 t = valid ? scene_entry(d, i) : make_float4(dt, 0.0f, 0.0f, 0.0f);
@@ -779,17 +777,10 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
     // pass, not after it.
     int s0 = 0, ns = 0, e0 = 0, nd = 0, g = 0, oe = -1;
     if (act) {
-      if (rec.w != -1) {
-        s0 = rec.y;
-        e0 = rec.z;
-        ns = rec.w & 0x7fff;
-        nd = (rec.w >> 15) & 0xffff;
-      } else {
-        s0 = d.sg_start[i];
-        ns = d.sg_start[i + 1] - s0;
-        e0 = d.dg_start[i];
-        nd = d.dg_start[i + 1] - e0;
-      }
+      s0 = d.sg_start[i];
+      ns = d.sg_start[i + 1] - s0;
+      e0 = d.dg_start[i];
+      nd = d.dg_start[i + 1] - e0;
       g = gl < ns ? s0 + gl : (gl < ns + nd ? d.dg_idx[e0 + (gl - ns)] : 0);
       oe = gl >= ns && gl < ns + nd ? d.dg_other[e0 + (gl - ns)] : -1;
     }
@@ -1434,25 +1425,6 @@ __device__ __noinline__ bool ph_color_dataflow(const Dev& d, int gtid, int gsize
   return true;
 }
 
-// Body record of one position of color_bodies, for the flag sweep: (body,
-// first static group, first dynamic incidence, w) with w = static groups |
-// dynamic incidences << 15 | (static body) << 31, or w = -1 when the counts
-// do not fit (the sweep then reads the ranges itself).  One load gives a
-// chunk everything it needs to start its group loads.
-__device__ __forceinline__ int4 chunk_rec_of(const Dev& d, int i) {
-  int s0 = d.sg_start[i], ns = d.sg_start[i + 1] - s0;
-  int e0 = d.dg_start[i], nd = d.dg_start[i + 1] - e0;
-  bool stat = d.x[i].w <= 0.0f;  // mass: constant
-  int w = (ns < 32767 && nd < 65536) ? (ns | (nd << 15) | (stat ? (int)0x80000000 : 0)) : -1;
-  return make_int4(i, s0, e0, w);
-}
-
-// No recolor this substep: color_bodies is unchanged (or was written by the
-// host), but the incidence ranges are new; rebuild the records by position.
-__device__ void ph_chunk_recs(const Dev& d, int gtid, int gsize) {
-  for (int p = gtid; p < d.nb; p += gsize) d.chunk_rec[p] = chunk_rec_of(d, d.color_bodies[p]);
-}
-
 // Bucketing of bodies by color.  Within a color, bodies come in four work
 // buckets, heaviest first: more than 24, 17-24, 9-16 and at most 8 incident
 // groups, i.e. by the lane rounds a body takes at 8 lanes.  The longest jobs
@@ -1546,7 +1518,6 @@ __device__ void ph_bucket_place(const Dev& d) {
         int off = run[key];
         for (int u = 0; u < w; ++u) off += wc[u][key];
         d.color_bodies[off + rank] = i;
-        d.chunk_rec[off + rank] = chunk_rec_of(d, i);
       }
       __syncthreads();
       if (threadIdx.x < NKEY) {
@@ -1600,8 +1571,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
   ph_mlp_prelude(d, gtid, gsize);
   if (spec) ph_color_dataflow(d, gtid, gsize);
   SYNC(PH_GATE_PRELUDE);
-  const bool recolor = recolor_needed(d);
-  if (recolor) {
+  if (recolor_needed(d)) {
     if (spec) {
       if (gtid == 0) d.ctr->recolored = 1;
     } else {
@@ -1636,7 +1606,6 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
     d.ctr->recolored = 0;
   }
   ph_predict<BATCHED>(d, gtid, gsize);
-  if (!recolor) ph_chunk_recs(d, gtid, gsize);  // with a recolor, ph_bucket_place wrote them
   SYNC(PH_PREDICT);
   int iters = P.iterations;
   // batched scenes: one pass beyond the most iterations, where each scene
