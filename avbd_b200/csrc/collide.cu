@@ -119,12 +119,9 @@ __global__ void k_morton(const __grid_constant__ Dev d) {
 }
 
 // ---------------------------------------------------------------------------
-// Device-wide exclusive scan (three launches).  Chunk = 2048 ints per block.
-// out[n] receives the total.
+// Device-wide exclusive scan (three launches).  SCAN_CHUNK ints per block
+// (common.cuh).  out[n] receives the total.
 // ---------------------------------------------------------------------------
-#define SCAN_T 256
-#define SCAN_V 8
-#define SCAN_CHUNK (SCAN_T * SCAN_V)
 
 __device__ __forceinline__ int warp_incl_scan(int v) {
 #pragma unroll

@@ -1,6 +1,6 @@
 // Shared device definitions for the B200 Solver6DOF substep.
 //
-// Data model (see DESIGN.md for the full table):
+// Data model:
 //  * bodies are SoA float4 arrays (x.xyz + mass, q, v, w, ...);
 //  * constraints are stored as *contact groups*: a normal row plus its two
 //    friction rows (floor corner or box-box contact), a 1-row frictionless
@@ -15,6 +15,13 @@
 #include "../../include/avbd6.h"
 
 namespace avbd {
+
+// Device-wide exclusive scan (collide.cu: k_scan_reduce / k_scan_parts /
+// k_scan_down): SCAN_T threads per block, SCAN_V ints per thread, so one
+// block covers SCAN_CHUNK ints and writes one block partial.
+#define SCAN_T 256
+#define SCAN_V 8
+#define SCAN_CHUNK (SCAN_T * SCAN_V)
 
 // Group kinds.  The row types they carry are those of solver_6dof.py:31-34.
 enum : int { KIND_FLOOR = 0, KIND_PIN = 1, KIND_BOX = 2 };

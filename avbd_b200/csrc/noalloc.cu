@@ -15,6 +15,12 @@
 // threads) race on it and give wrong results, so serialise them.  Nothing in
 // it needs clearing between calls: each scan writes every partial it later
 // reads.
+//
+// The array's device address is looked up once per device, with that device
+// current, on the first call made there (so make that first call before any
+// stream capture).  cudaDeviceReset unloads the library's module; its array
+// may then sit elsewhere, so do not call this entry point after a
+// cudaDeviceReset in the same process.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -34,8 +40,9 @@ using namespace avbd;
 
 namespace {
 
-constexpr int kChunk = 2048;     // ints per block of the scan kernels (256 threads x 8)
-constexpr int kMaxParts = 4096;  // block partials the static scratch holds
+constexpr int kChunk = SCAN_CHUNK;  // ints per block of the scan kernels (common.cuh)
+static_assert(kChunk == SCAN_T * SCAN_V, "the scan kernels cover SCAN_T x SCAN_V ints per block");
+constexpr int kMaxParts = 4096;     // block partials the static scratch holds
 constexpr int kMaxN = kMaxParts * kChunk - 1;  // 8,388,607 ints
 
 // The scratch: block partial sums plus the total (kMaxParts + 1 ints).
@@ -81,9 +88,9 @@ extern "C" int avbd_exclusive_scan_noalloc(const int* in, int* out, int n, void*
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int np = (n + kChunk) / kChunk;  // blocks covering index n (the total)
-  k_scan_reduce<<<np, 256, 0, st>>>(in, n, nullptr, part);
-  k_scan_parts<<<1, 256, 0, st>>>(part, np);
-  k_scan_down<<<np, 256, 0, st>>>(in, out, n, nullptr, part, np, nullptr);
+  k_scan_reduce<<<np, SCAN_T, 0, st>>>(in, n, nullptr, part);
+  k_scan_parts<<<1, SCAN_T, 0, st>>>(part, np);
+  k_scan_down<<<np, SCAN_T, 0, st>>>(in, out, n, nullptr, part, np, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error_text("avbd_exclusive_scan_noalloc: launch", e);

@@ -190,8 +190,9 @@ int avbd_read_phase_marks(AvbdCtx* ctx, long long* t_ns, int* phase, int cap, vo
  * library, so n is limited to 8,388,607 (larger n returns AVBD_E_INVALID).
  * The first call on a device looks the array up (cudaGetSymbolAddress); make
  * that first call before any stream capture.  All calls on a device share the
- * array: calls that overlap on the GPU race, so serialise them.  `in` and
- * `out` are device pointers; asynchronous on `stream`. */
+ * array: calls that overlap on the GPU race, so serialise them.  The looked-up
+ * address is kept for the process: do not call this after cudaDeviceReset.
+ * `in` and `out` are device pointers; asynchronous on `stream`. */
 int avbd_exclusive_scan_noalloc(const int* in, int* out, int n, void* stream);
 
 /* ---------------------------------------------------------------------

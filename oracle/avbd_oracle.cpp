@@ -16,8 +16,8 @@
 // float copies of the pose, exactly like the reference, so that its discrete
 // outputs can be compared bit-for-bit with the GPU.
 //
-// Defined semantics where the reference is order dependent (documented in
-// DESIGN.md):
+// Defined semantics where the reference is order dependent (the GPU kernels
+// implement the same ones):
 //  * pair order: pairs are sorted by (min body, max body); rows are emitted in
 //    pair order, contacts in manifold order;
 //  * coloring: every Jones-Plassmann / speculative round reads the previous

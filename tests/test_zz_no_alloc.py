@@ -48,3 +48,26 @@ def test_noalloc_scan_rejects_oversized_input():
     lib = _lib.load()
     r = lib.avbd_exclusive_scan_noalloc(ctypes.c_void_p(1), ctypes.c_void_p(1), 8388608, None)
     assert r < 0 and b"8388607" in lib.avbd_last_error()
+
+
+@pytest.mark.parametrize("n", [0, 1, 2048 * 300, 8388607])
+def test_noalloc_scan_multi_block_sizes(n):
+    """Sizes that reach the scan's carry between batches of 256 block
+    partials (2048 x 300 ints: 301 partials) and the largest size the fixed
+    scratch holds (8,388,607 ints: 4096 partials, the total in its last
+    slot), checked against numpy twice in a row."""
+    from avbd_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(n)
+    vals = rng.integers(0, 200, size=max(n, 1), dtype=np.int32)[:n]  # total < 2^31
+    src = torch.from_numpy(vals.copy()).cuda() if n else torch.zeros(1, dtype=torch.int32, device="cuda")
+    want = np.zeros(n + 1, np.int64)
+    want[1:] = np.cumsum(vals, dtype=np.int64)
+    stream = torch.cuda.current_stream()
+    for call in range(2):
+        out = torch.full((n + 1,), -7, dtype=torch.int32, device="cuda")
+        r = lib.avbd_exclusive_scan_noalloc(ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(out.data_ptr()), n,
+                                            ctypes.c_void_p(stream.cuda_stream))
+        assert r == 0, lib.avbd_last_error()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy().astype(np.int64), want, err_msg=f"n={n} call {call}")
