@@ -12,9 +12,12 @@ time of the timed steps (CUDA events on the solver's stream, L2 flushed between
 steps outside the events); with torchrun, N independent replicas (one pile per
 GPU, no collective in the loop) and the max time over ranks.
 
-`--impl reference` times the CPU restatement of the reference algorithm (the
-reference's own Warp CPU path cannot be installed here) on all host cores, on a
-bounded sample of the workload (a 20x20x10 tile of the same pile distribution).
+`--impl reference` times the CPU port of the reference substep (the oracle:
+the C++ restatement, which reproduces the reference's own kernels bit for bit;
+the reference's Warp CPU path itself cannot be installed here) on all host
+cores, on the same settled 100k pile (state prepared untimed on the GPU), one
+substep per step; a 20x20x10 tile on all cores and on one core is reported
+beside it.
 """
 
 from __future__ import annotations
@@ -125,9 +128,14 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle (C++ restatement, OpenMP) on a tile of the pile.
+# CPU baseline: the oracle (C++ restatement of the reference substep, FP32,
+# OpenMP), which reproduces the reference's own kernels bit for bit
+# (tests/test_reference_pin.py).
 # ---------------------------------------------------------------------------
-def cpu_rate(steps: int, warmup: int, threads: int, settle: int = 120) -> dict:
+def cpu_rate(steps: int, warmup: int, threads: int, settle: int = 120, also_threads=()) -> dict:
+    """The port on a 20x20x10 tile of the pile, settled on the CPU with all
+    `threads`; then `steps` frames are timed with `threads` and with each
+    count in `also_threads` (reported under "by_threads")."""
     from avbd_b200 import scenes
     from oracle.oracle import OracleSolver6DOF
     s = OracleSolver6DOF(precision="float32", threads=threads, **PARAMS)
@@ -135,32 +143,104 @@ def cpu_rate(steps: int, warmup: int, threads: int, settle: int = 120) -> dict:
     for _ in range(settle + warmup):
         s.step()
     nb = dyn_bodies(s)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        s.step()
-    dt = time.perf_counter() - t0
     c = s.counts()
+    by = {}
+    for th in (threads, *also_threads):
+        s.threads = th
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            s.step()
+        by[th] = time.perf_counter() - t0
+    s.threads = threads
+    dt = by[threads]
     return {"value": nb * PARAMS["substeps"] * steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": (f"{SAMPLE['nx']}x{SAMPLE['nz']}x{SAMPLE['ny']} tile of the pile ({nb} boxes, "
                        f"{c['n_rows'] - c['n_static']} dynamic rows), settled {settle} frames, "
                        f"{steps} timed frames; FP32 C++ restatement of the reference substep"),
-            "seconds": dt}
+            "seconds": dt, "by_threads": {str(th): nb * PARAMS["substeps"] * steps / t for th, t in by.items()}}
+
+
+def settled_pile_state(settle: int, size=None) -> dict:
+    """The benchmark pile settled on the GPU by this package (untimed input
+    preparation: settling 100k boxes for 240 frames would take the port the
+    better part of an hour).  Returns the Solver6DOF state_dict."""
+    from avbd_b200 import Solver6DOF, scenes
+    s = Solver6DOF(**PARAMS)
+    scenes.pile(s, **(size or FULL))
+    for _ in range(settle):
+        s._enqueue_step()
+    s._after_frame()
+    sd = s.state_dict()
+    del s
+    return sd
+
+
+def port_full_rate(sd: dict, substeps: int, warmup: int, threads: int, size=None, settle: int = 240) -> dict:
+    """The port on the full settled pile: the state is loaded into the
+    oracle's FP32 build, `warmup` substeps run untimed, then `substeps`
+    substeps are timed (one substep is a bounded sample of one frame)."""
+    from avbd_b200 import scenes
+    from oracle.oracle import OracleSolver6DOF
+    size = size or FULL
+    s = OracleSolver6DOF(precision="float32", threads=threads, **PARAMS)
+    scenes.pile(s, **size)
+    s._flush()
+    s.set_bodies(sd["x"], sd["q"], sd["v"], sd["w"], sd["pv"], sd["pw"])
+    s.set_static_rows(sd["row_lam"], sd["row_pen"], sd["row_active"], sd["row_was"])
+    s.set_cache(sd["cache_abc"], sd["cache_state"])
+    s.set_colors(sd["colors"], sd["n_colors"], sd["color_dirty"])
+    for _ in range(warmup):
+        s.substep()
+    nb = dyn_bodies(s)
+    t0 = time.perf_counter()
+    for _ in range(substeps):
+        s.substep()
+    dt = time.perf_counter() - t0
+    c = s.counts()
+    return {"value": nb * substeps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"full {size['nx']}x{size['nz']}x{size['ny']} pile ({nb} boxes, "
+                       f"{c['n_rows'] - c['n_static']} dynamic rows, {c['n_pairs']} pairs) settled {settle} frames "
+                       f"(state prepared untimed on the GPU), {substeps} timed substeps after {warmup} warm-up "
+                       "substeps; FP32 C++ restatement of the reference substep"),
+            "seconds": dt, "dyn_rows": c["n_rows"] - c["n_static"]}
 
 
 def run_reference(args) -> None:
+    """The reference arm: the port of the reference substep on the host
+    cores, on the same settled 100k pile as the GPU arm (one substep per
+    step), with the tile sample on all cores and on one core beside it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    r = cpu_rate(args.steps, args.warmup, threads)
+    extra = {}
+    try:
+        import torch
+        have_gpu = torch.cuda.is_available()
+    except Exception:
+        have_gpu = False
+    if have_gpu:
+        sd = settled_pile_state(args.settle)
+        r = port_full_rate(sd, args.steps, args.warmup, threads, settle=args.settle)
+        same = True
+        workload = ("pile 100x100x10 (100000 OBBs, he U[0.2,0.4], 200 corner pins fracture 5e4), dt 1/60, "
+                    "4 substeps, 10 iterations + post-stab, JP coloring; one substep per step")
+    else:  # no GPU to prepare the settled state: the tile alone
+        r = cpu_rate(args.steps, args.warmup, threads)
+        same = False
+        extra["same_config_reason"] = "no GPU to prepare the settled 100k pile; 20x20x10 tile timed instead"
+        workload = "pile tile 20x20x10 (bounded sample)"
+    tile = cpu_rate(3, 2, threads, also_threads=(1,))
+    extra["tile"] = {"sample": tile["sample"], "body_substeps_per_s_by_threads": tile["by_threads"]}
     line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / max(1, args.steps),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "pile (OBB pile, 4 substeps x (10+1) iterations, JP coloring): bounded tile sample",
-                       "sample": r["sample"]},
+            "same_config": same,
+            "config": {"workload": workload, "sample": r["sample"]},
             "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": r["sample"]},
-            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            **extra}
     print(json.dumps(line), flush=True)
 
 
@@ -255,7 +335,7 @@ def run_gpu(args) -> None:
         s._enqueue_step()
     s._after_frame()
     tuned = None
-    if not (args.no_tune or args.group_size or args.blocks_per_sm or args.sweep):
+    if args.tune and not (args.group_size or args.blocks_per_sm or args.sweep):
         from avbd_b200.autotune import autotune
         tuned = autotune(s)  # launch shape for this scene; the scene state is restored
     for _ in range(args.warmup):
@@ -378,10 +458,9 @@ def run_gpu(args) -> None:
             for r in tuned["table"]}
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        # the same sample as the reference arm: a settled tile (fewer settle
-        # frames would time a tile whose boxes are still falling, with a
-        # third of the contact rows)
-        cb = cpu_rate(steps=3, warmup=3, threads=threads, settle=120)
+        # the port on this run's own settled pile (the GPU state loaded into
+        # the oracle), a few substeps: the same configuration as `value`
+        cb = port_full_rate(s.state_dict(), substeps=3, warmup=1, threads=threads, size=size, settle=args.settle)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0 and not args.no_warm_start:
         line["warm_start"] = warm_start_eval()
@@ -515,11 +594,14 @@ def main():
     ap.add_argument("--small", action="store_true", help="40x40x10 pile (profiling captures)")
     ap.add_argument("--profile", action="store_true", help="cudaProfilerStart/Stop around the timed steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--group-size", type=int, default=0, help="lanes per body (0 = autotuned)")
-    ap.add_argument("--blocks-per-sm", type=int, default=0, help="solve CTAs per SM (0 = autotuned)")
+    ap.add_argument("--group-size", type=int, default=0, help="lanes per body (0 = the solver default)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="solve CTAs per SM (0 = the solver default)")
     ap.add_argument("--sweep", default="", choices=["", "barrier", "barrier-adaptive", "flags"],
-                    help="color-pass ordering (empty = autotuned)")
-    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+                    help="color-pass ordering (empty = the solver default)")
+    ap.add_argument("--tune", action="store_true",
+                    help="run the launch-shape autotuner before timing and report its table (the default "
+                         "times Solver6DOF's own default shape, as a drop-in user gets it)")
+    ap.add_argument("--no-tune", action="store_true", help="batched bench: skip the autotuner")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start evaluation")
     ap.add_argument("--row-capacity", type=int, default=0, help="initial dynamic-row pool (0 = reference size)")
     ap.add_argument("--batched", action="store_true", help="512 batched scenes vs one scene at a time")
