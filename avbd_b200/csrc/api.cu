@@ -469,7 +469,12 @@ int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {
   out->n_mlp_applied = h.n_mlp_applied;
   out->n_mlp_fallback = h.n_mlp_fallback;
   out->n_mlp_reverted = h.n_mlp_reverted;
-  for (int k = 0; k < 64; ++k) out->viol_contact[k] = h.vc_cnt[k] > 0 ? h.vc_sum[k] / (float)h.vc_cnt[k] : 0.0f;
+  for (int k = 0; k < 64; ++k) {
+    unsigned b = h.vc_max_bits[k];
+    float f;
+    memcpy(&f, &b, sizeof f);
+    out->viol_contact[k] = f;
+  }
   for (int k = 0; k < 64; ++k) {
     unsigned b = h.viol_bits[k];
     float f;

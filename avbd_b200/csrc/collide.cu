@@ -54,7 +54,7 @@ __global__ void k_begin_substep(const __grid_constant__ Dev d) {
     for (int k = 0; k < BAR_SUB; ++k) c->bar_sub[k][0] = 0;
     for (int k = 0; k < 64; ++k) {
       c->viol_bits[k] = 0;
-      c->vc_sum[k] = 0.0f;
+      c->vc_max_bits[k] = 0u;
       c->vc_cnt[k] = 0;
     }
     int* b = (int*)d.bounds;

@@ -138,8 +138,8 @@ struct DevCounters {
   int round_unc[2];  // uncolored counts of alternate coloring rounds
   int work_ctr[4];   // color passes: next chunk to hand out (pass q uses q & 3)
   int pad4[26];
-  float vc_sum[64];  // per-iteration violation sum over box-box contact groups
-  int vc_cnt[64];    // and their count (record_violation)
+  unsigned vc_max_bits[64];  // per-iteration max violation over box-box contact groups (float bits)
+  int vc_cnt[64];            // and their count (record_violation)
 };
 #define BAR_SUB 16
 

@@ -395,7 +395,7 @@ __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3
     d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
     d.g_flags[g] = fl;
     if (kind == KIND_BOX && (fl & FL_ACT0)) {
-      csum += viol;
+      csum = fmaxf(csum, viol);
       ++ccnt;
     }
   }
@@ -574,18 +574,18 @@ struct PassMode {
 };
 
 // Folds a warp's violation statistics of iteration `slot` into the
-// counters: the max over all rows, and the sum / count over box-box contact
-// groups (their mean is the contact-row statistic).
-__device__ __forceinline__ void record_violation(const Dev& d, int slot, float vmax, float csum, int ccnt) {
+// counters: the max over all rows, and the max and count over box-box
+// contact groups (cmax: the rows a contact warm start sets).
+__device__ __forceinline__ void record_violation(const Dev& d, int slot, float vmax, float cmax, int ccnt) {
   for (int o = 16; o > 0; o >>= 1) {
     vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-    csum += __shfl_xor_sync(0xffffffffu, csum, o);
+    cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
     ccnt += __shfl_xor_sync(0xffffffffu, ccnt, o);
   }
   if (lane_id() == 0) {
     if (vmax > 0.0f) atomicMax(&d.ctr->viol_bits[slot], __float_as_uint(vmax));
     if (ccnt > 0) {
-      atomicAdd(&d.ctr->vc_sum[slot], csum);
+      if (cmax > 0.0f) atomicMax(&d.ctr->vc_max_bits[slot], __float_as_uint(cmax));
       atomicAdd(&d.ctr->vc_cnt[slot], ccnt);
     }
   }
@@ -1806,7 +1806,7 @@ __global__ void k_reset(const __grid_constant__ Dev d) {
     for (int k = 0; k < BAR_SUB; ++k) c->bar_sub[k][0] = 0;
     for (int k = 0; k < 64; ++k) {
       c->viol_bits[k] = 0;
-      c->vc_sum[k] = 0.0f;
+      c->vc_max_bits[k] = 0u;
       c->vc_cnt[k] = 0;
     }
   }

@@ -166,30 +166,16 @@ class WarmStartMLP:
 
 
 # ---- data collection and evaluation ----------------------------------------
-def _cache_lookup(sd: dict, a: np.ndarray, b: np.ndarray, c: np.ndarray):
-    """Rows of sd's contact cache holding keys (min(a,b), max(a,b), c);
-    -1 where the cache has no entry."""
-    abc = np.asarray(sd["cache_abc"], np.int64)
-    if abc.shape[0] == 0:
-        return np.full(len(a), -1, np.int64)
-    key = (abc[:, 0] << 26) | (abc[:, 1] << 2) | abc[:, 2]
-    order = np.argsort(key)
-    ks = key[order]
-    want = (np.minimum(a, b).astype(np.int64) << 26) | (np.maximum(a, b).astype(np.int64) << 2) | c.astype(np.int64)
-    pos = np.clip(np.searchsorted(ks, want), 0, len(ks) - 1)
-    return np.where(ks[pos] == want, order[pos], -1)
-
-
-def collect_cold_start(solver):
-    """Training samples from the solver's current state: the features of
-    every box-box contact, labelled with the state the contact cache holds
-    for it -- the warm start the learned start has to stand in for.  The
-    features come from one substep run with the cache emptied (so every
-    contact is logged as new); the solver's state is restored afterwards.
-    Returns (features [n, 20], targets [n, 4]) for the contacts found in the
-    cache."""
+def collect_converged(solver, iterations: int = 50):
+    """Training samples from the solver's current state: one substep of
+    `iterations` iterations is run from the plain zero start with the contact
+    cache emptied, so every contact is new and logged with its 20 features
+    at emission; each contact is labelled with the state it converged to --
+    (lambda n/t1/t2, penalty n) at the end of that substep.  The solver's
+    state and iteration count are restored afterwards.  Returns (features
+    [n, 20], targets [n, 4])."""
     sd = solver.state_dict()
-    log0 = solver.log_new_contacts
+    log0, it0 = solver.log_new_contacts, solver.iterations
     ws = solver.warm_start
     en0 = ws.enabled if ws is not None else None
     if ws is not None:
@@ -197,29 +183,27 @@ def collect_cold_start(solver):
     solver.log_new_contacts = True  # may re-flush (bodies kept): reload the state
     solver.load_state_dict(sd)
     solver.clear_contact_cache()
-    solver.substep()
-    feat, gid = solver.new_contact_log()
-    body = solver._g_body[torch.as_tensor(gid.astype(np.int64), device=solver.device)].cpu().numpy()
-    meta = solver._g_meta[torch.as_tensor(gid.astype(np.int64), device=solver.device)].cpu().numpy()
-    row = _cache_lookup(sd, body[:, 0], body[:, 1], (meta >> 4) & 3)
-    solver.log_new_contacts = log0
-    if ws is not None:
-        ws.enabled = en0
-    solver.load_state_dict(sd)
-    hit = row >= 0
-    st = np.asarray(sd["cache_state"], np.float32)[row[hit]]
-    lam = st[:, 0:3]
-    pen = st[:, 3:6]
-    return feat[hit], targets(lam, pen)
+    solver.iterations = int(iterations)
+    try:
+        solver.substep()
+        feat, gid = solver.new_contact_log()
+        lam, pen = solver.group_state(gid)
+    finally:
+        solver.iterations = it0
+        solver.log_new_contacts = log0
+        if ws is not None:
+            ws.enabled = en0
+        solver.load_state_dict(sd)
+    return feat, targets(lam[:, 0:3], pen[:, 0:3])
 
 
 def cold_start_violation(solver, iterations: int = 64, learned: bool = True, clear_cache: bool = True):
-    """Max constraint violation after each iteration of one substep from the
-    solver's current state -- with the contact cache emptied (every contact
-    new) unless `clear_cache` is False, with or without the learned warm
-    start -- and the substep's stats (with the per-iteration mean violation
-    of the box-box contacts as stats["contact_violation"]).  The state is
-    restored afterwards."""
+    """Max constraint violation over all rows after each iteration of one
+    substep from the solver's current state -- with the contact cache emptied
+    (every contact new) unless `clear_cache` is False, with or without the
+    learned warm start -- and the substep's stats (with the per-iteration max
+    violation over the box-box contacts as stats["contact_violation"]).  The
+    state is restored afterwards."""
     sd = solver.state_dict()
     it0, rv0 = solver.iterations, solver.record_violation
     ws = solver.warm_start

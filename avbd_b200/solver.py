@@ -956,8 +956,9 @@ class Solver6DOF:
         return np.array(s.viol[: s.n_viol], np.float64)
 
     def contact_violation_history(self) -> np.ndarray:
-        """Mean violation of the box-box contacts after each iteration of the
-        last substep (record_violation)."""
+        """Max violation over the box-box contacts (the rows a contact warm
+        start sets) after each iteration of the last substep
+        (record_violation)."""
         s = self._stats
         return np.array(s.viol_contact[: s.n_viol], np.float64)
 

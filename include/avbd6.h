@@ -120,7 +120,7 @@ typedef struct AvbdStats {
   int n_mlp_reverted; /* learned starts reset to the zero start at their first
                          dual update because the contact separated (the
                          predicted force raised the complementarity residual) */
-  float viol_contact[64]; /* per-iteration mean violation of box-box contacts */
+  float viol_contact[64]; /* per-iteration max violation over box-box contacts */
 } AvbdStats;
 
 typedef struct AvbdCtx AvbdCtx;
