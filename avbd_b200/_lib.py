@@ -8,6 +8,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libavbd6.so")
 
+MAX_VIOL_ITERS = 256  # AVBD_MAX_VIOL_ITERS (include/avbd6.h)
 AVBD_ERR_BARRIER_TIMEOUT = 1
 AVBD_ERR_HASH_FULL = 2
 AVBD_ERR_PAIR_OVERFLOW = 4
@@ -43,9 +44,9 @@ class AvbdStats(C.Structure):
                 ("n_colors", C.c_int), ("recolored", C.c_int), ("conflicts", C.c_int), ("err", C.c_int),
                 ("err_where", C.c_int), ("n_cache_hits", C.c_int), ("n_new_contacts", C.c_int),
                 ("max_dg", C.c_int), ("n_viol", C.c_int), ("epoch", C.c_uint), ("graph_state", C.c_int),
-                ("capture_err", C.c_int), ("kernels_launched", C.c_longlong), ("viol", C.c_float * 64),
+                ("capture_err", C.c_int), ("kernels_launched", C.c_longlong), ("viol", C.c_float * MAX_VIOL_ITERS),
                 ("n_new_logged", C.c_int), ("n_mlp_applied", C.c_int), ("n_mlp_fallback", C.c_int), ("n_mlp_reverted", C.c_int),
-                ("viol_contact", C.c_float * 64)]
+                ("viol_contact", C.c_float * MAX_VIOL_ITERS)]
 
 # Learned warm-start network sizes (avbd6.h AVBD_MLP_*).
 MLP_IN = 20
@@ -93,11 +94,16 @@ def load():
     L.avbd_mlp_scratch_bytes.restype = sz
     L.avbd_mlp_loss_grad.argtypes = [vp, vp, vp, i, vp, vp, vp, sz, vp]
     L.avbd_mlp_adam.argtypes = [vp, vp, vp, vp, i, C.c_float, C.c_float, C.c_float, C.c_float, vp]
+    L.avbd_profile_next_substep.argtypes = [vp]
+    L.avbd_collision_profile.argtypes = [vp, C.POINTER(C.c_float), i]
+    L.avbd_collision_stage.argtypes = [vp, i]
+    L.avbd_collision_stage.restype = C.c_char_p
     for name in ("avbd_layout", "avbd_create", "avbd_destroy", "avbd_set_params", "avbd_reset_state",
                  "avbd_mark_color_dirty", "avbd_substep", "avbd_step", "avbd_read_stats",
                  "avbd_count_color_conflicts", "avbd_cache_load", "avbd_cache_load_keys", "avbd_clear_errors",
                  "avbd_step_ms",
-                 "avbd_read_phase_marks", "avbd_mlp_pack", "avbd_mlp_infer", "avbd_mlp_loss_grad", "avbd_mlp_adam"):
+                 "avbd_read_phase_marks", "avbd_mlp_pack", "avbd_mlp_infer", "avbd_mlp_loss_grad", "avbd_mlp_adam",
+                 "avbd_profile_next_substep", "avbd_collision_profile"):
         getattr(L, name).restype = i
     _lib = L
     return L
@@ -116,7 +122,8 @@ EXPORTED = ["avbd_num_arrays", "avbd_array_name", "avbd_layout", "avbd_create", 
             "avbd_read_stats", "avbd_count_color_conflicts", "avbd_cache_load", "avbd_cache_load_keys",
             "avbd_clear_errors",
             "avbd_step_ms", "avbd_read_phase_marks", "avbd_exclusive_scan_noalloc", "avbd_mlp_pack",
-            "avbd_mlp_infer", "avbd_mlp_scratch_bytes", "avbd_mlp_loss_grad", "avbd_mlp_adam", "avbd_last_error"]
+            "avbd_mlp_infer", "avbd_mlp_scratch_bytes", "avbd_mlp_loss_grad", "avbd_mlp_adam", "avbd_last_error",
+            "avbd_profile_next_substep", "avbd_collision_profile", "avbd_collision_stage"]
 
 PHASES = ["start", "gate+prelude", "color reset", "color rounds", "bucket", "predict", "primal", "dual",
           "collect"]

@@ -108,6 +108,7 @@ struct AvbdCtx {
   int num_sms;
   int coll_grid;
   int solve_grid, solve_block, solve_variant;
+  int sweep_grid;  // CTAs of the standalone flag-sweep launch (0: the sweep runs inside the persistent kernel)
   // parts: 0 = collision with an LBVH rebuild, 1 = solve, 2 = collision
   // that refits the previous tree
   cudaGraphExec_t exec[3];
@@ -122,6 +123,9 @@ struct AvbdCtx {
   long long substeps_done;
   float cur_dt;
   cudaEvent_t ev[3];
+  StageTimer timer;      // stage events of a profiled collision pipeline
+  int profile_next;      // the next substep runs its collision pipeline eagerly, timed
+  int profile_ready;     // timer holds a completed profile
 };
 
 extern "C" {
@@ -228,6 +232,7 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   c->P.use_graph = 1;
   c->P.persistent = 1;
   for (int k = 0; k < 3; ++k) cudaEventCreate(&c->ev[k]);
+  for (int k = 0; k < StageTimer::kMax; ++k) cudaEventCreate(&c->timer.ev[k]);
   *out = c;
   return AVBD_OK;
 }
@@ -237,6 +242,8 @@ int avbd_destroy(AvbdCtx* c) {
   for (int part = 0; part < 3; ++part) drop_graph(c, part);
   for (int k = 0; k < 3; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  for (int k = 0; k < StageTimer::kMax; ++k)
+    if (c->timer.ev[k]) cudaEventDestroy(c->timer.ev[k]);
   delete c;
   return AVBD_OK;
 }
@@ -278,7 +285,8 @@ static void fill_devparams(AvbdCtx* c, float dt_sub) {
 
 int avbd_set_params(AvbdCtx* c, const AvbdParams* p, void* stream) {
   if (!c || !p) return fail(AVBD_E_INVALID, "null argument");
-  if (p->iterations < 0 || p->iterations > 64 || p->substeps < 1) return fail(AVBD_E_INVALID, "bad iterations/substeps");
+  if (p->iterations < 0 || p->iterations > AVBD_MAX_VIOL_ITERS || p->substeps < 1)
+    return fail(AVBD_E_INVALID, "iterations must be in [0, 256] and substeps >= 1");
   c->P = *p;
   c->cur_dt = p->dt / (float)p->substeps;
   fill_devparams(c, c->cur_dt);
@@ -291,6 +299,7 @@ int avbd_set_params(AvbdCtx* c, const AvbdParams* p, void* stream) {
   int occ = solve_occupancy(256, c->solve_variant);
   int b = want < occ ? want : occ;
   c->solve_grid = c->num_sms * (b > 0 ? b : 1);
+  c->sweep_grid = p->flag_sweep ? sweep_grid_size(p->group_size, c->d.n_scenes > 0, c->num_sms) : 0;
   return AVBD_OK;
 }
 
@@ -318,7 +327,8 @@ static cudaError_t enqueue_part(AvbdCtx* c, int part, cudaStream_t st) {
     launch_collision(c->d, c->P, c->dims, c->coll_grid, st, part == 0);
     e = cudaGetLastError();
   } else {
-    e = launch_solve(c->d, c->P, c->P.persistent, c->solve_grid, c->solve_block, st, c->solve_variant);
+    e = launch_solve(c->d, c->P, c->P.persistent, c->solve_grid, c->solve_block, st, c->solve_variant,
+                     c->sweep_grid);
   }
   c->part_kernels[part] = (int)(g_kernel_launches - before);
   return e;
@@ -329,8 +339,9 @@ static void part_key(AvbdCtx* c, int part, int key[4]) {
     key[0] = c->P.self_collide; key[1] = c->coll_grid; key[2] = 0; key[3] = 0;
   } else {
     key[0] = c->P.persistent + 10 * c->solve_variant; key[1] = c->solve_grid;
-    key[2] = c->P.persistent ? 0 : c->P.iterations + 100 * c->P.post_stabilize;
-    key[3] = c->P.persistent ? 0 : c->P.coloring_mode;
+    key[2] = c->P.persistent ? (c->P.flag_sweep ? 1000 + c->P.group_size : 0)
+                             : c->P.iterations + 100 * c->P.post_stabilize;
+    key[3] = c->P.persistent ? c->sweep_grid : c->P.coloring_mode;
   }
 }
 
@@ -394,7 +405,18 @@ static int run_substep(AvbdCtx* c, cudaStream_t st) {
   c->bvh_age = !collide ? 0 : (rebuild ? 1 : c->bvh_age + 1);
   c->last_coll_part = part;
   cudaEventRecord(c->ev[0], st);
-  cudaError_t e = run_part(c, part, st);
+  cudaError_t e;
+  if (c->profile_next) {  // eager launches with a stage event after each
+    c->timer.n = 0;
+    g_stage_timer = &c->timer;
+    e = enqueue_part(c, part, st);
+    g_stage_timer = nullptr;
+    c->kernels_launched += c->part_kernels[part];
+    c->profile_next = 0;
+    c->profile_ready = 1;
+  } else {
+    e = run_part(c, part, st);
+  }
   if (e != cudaSuccess) return fail(AVBD_E_CUDA, "collision launch", e);
   cudaEventRecord(c->ev[1], st);
   e = run_part(c, 1, st);
@@ -469,13 +491,13 @@ int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {
   out->n_mlp_applied = h.n_mlp_applied;
   out->n_mlp_fallback = h.n_mlp_fallback;
   out->n_mlp_reverted = h.n_mlp_reverted;
-  for (int k = 0; k < 64; ++k) {
+  for (int k = 0; k < AVBD_MAX_VIOL_ITERS; ++k) {
     unsigned b = h.vc_max_bits[k];
     float f;
     memcpy(&f, &b, sizeof f);
     out->viol_contact[k] = f;
   }
-  for (int k = 0; k < 64; ++k) {
+  for (int k = 0; k < AVBD_MAX_VIOL_ITERS; ++k) {
     unsigned b = h.viol_bits[k];
     float f;
     std::memcpy(&f, &b, 4);
@@ -544,6 +566,35 @@ int avbd_read_phase_marks(AvbdCtx* c, long long* t_ns, int* phase, int cap, void
 int avbd_count_color_conflicts(AvbdCtx* c, void* stream) {
   if (!c) return fail(AVBD_E_INVALID, "null ctx");
   return count_conflicts(c->d, (cudaStream_t)stream);
+}
+
+
+int avbd_profile_next_substep(AvbdCtx* c) {
+  if (!c) return fail(AVBD_E_INVALID, "null ctx");
+  c->profile_next = 1;
+  c->profile_ready = 0;
+  return AVBD_OK;
+}
+
+int avbd_collision_profile(AvbdCtx* c, float* ms, int cap) {
+  if (!c || (!ms && cap > 0)) return fail(AVBD_E_INVALID, "null argument");
+  if (!c->profile_ready) return fail(AVBD_E_INVALID, "no profiled substep has run");
+  int n = c->timer.n;
+  if (n < 1) return 0;
+  cudaError_t e = cudaEventSynchronize(c->timer.ev[n - 1]);
+  if (e != cudaSuccess) return fail(AVBD_E_CUDA, "profile events", e);
+  int k = 0;
+  for (; k + 1 < n && k < cap; ++k) {
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, c->timer.ev[k], c->timer.ev[k + 1]);
+    ms[k] = t;
+  }
+  return k;
+}
+
+const char* avbd_collision_stage(AvbdCtx* c, int i) {
+  if (!c || !c->profile_ready || i < 0 || i + 1 >= c->timer.n) return "";
+  return c->timer.name[i + 1];
 }
 
 }  // extern "C"

@@ -29,6 +29,12 @@ __device__ __forceinline__ float ord2f(int i) { return __int_as_float(i >= 0 ? i
 // Substep start: reset counters and the scene bounds used for Morton codes.
 // ---------------------------------------------------------------------------
 __global__ void k_begin_substep(const __grid_constant__ Dev d) {
+  if (blockIdx.x == 0 && d.prm->record_violation)  // per-iteration violation records of this substep
+    for (int k = threadIdx.x; k < AVBD_MAX_VIOL_ITERS; k += blockDim.x) {
+      d.ctr->viol_bits[k] = 0u;
+      d.ctr->vc_max_bits[k] = 0u;
+      d.ctr->vc_cnt[k] = 0;
+    }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     DevCounters* c = d.ctr;
     c->n_pairs_found = 0;
@@ -52,11 +58,6 @@ __global__ void k_begin_substep(const __grid_constant__ Dev d) {
     c->n_viol = 0;
     c->bar_count = 0;
     for (int k = 0; k < BAR_SUB; ++k) c->bar_sub[k][0] = 0;
-    for (int k = 0; k < 64; ++k) {
-      c->viol_bits[k] = 0;
-      c->vc_max_bits[k] = 0u;
-      c->vc_cnt[k] = 0;
-    }
     int* b = (int*)d.bounds;
     b[0] = b[1] = b[2] = 0x7fffffff;
     b[3] = b[4] = b[5] = (int)0x80000000;
@@ -977,36 +978,57 @@ __global__ void k_dg_clear(const __grid_constant__ Dev d) {
 // ---------------------------------------------------------------------------
 // Host-side launch sequence of the collision pipeline.
 // ---------------------------------------------------------------------------
+thread_local StageTimer* g_stage_timer = nullptr;
+
 void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int grid, cudaStream_t st, bool rebuild) {
+  stage_mark(st, "start");
   k_begin_substep<<<grid, 256, 0, st>>>(d);
+  stage_mark(st, "k_begin_substep");
   bool collide = P.self_collide && d.nb >= 2;
   if (!collide) {
     k_dg_clear<<<grid, 256, 0, st>>>(d);
+    stage_mark(st, "k_dg_clear");
     g_kernel_launches += 2;
     return;
   }
   k_aabb<<<grid, 256, 0, st>>>(d);
+  stage_mark(st, "k_aabb");
   if (rebuild) {
     k_morton<<<grid, 256, 0, st>>>(d);
+    stage_mark(st, "k_morton");
     radix_sort_launch(d, st);
+    stage_mark(st, "radix_sort");
     k_lbvh_build<<<grid, 256, 0, st>>>(d);
+    stage_mark(st, "k_lbvh_build");
   } else {
     k_lbvh_leaves<<<grid, 256, 0, st>>>(d);  // same topology, new leaf boxes
+    stage_mark(st, "k_lbvh_leaves");
   }
   k_lbvh_refit<<<grid, 256, 0, st>>>(d);
+  stage_mark(st, "k_lbvh_refit");
   k_lbvh_pack<<<grid, 256, 0, st>>>(d);
+  stage_mark(st, "k_lbvh_pack");
   k_bp_count<<<grid, 128, 0, st>>>(d);
+  stage_mark(st, "k_bp_count");
   scan_launch(d, d.up_cnt, d.pair_start, d.nb, nullptr, nullptr, st);
+  stage_mark(st, "scan_pair_offsets");
   k_bp_fill<<<grid, 128, 0, st>>>(d);
+  stage_mark(st, "k_bp_fill");
   k_narrow<<<grid, 128, 0, st>>>(d);
+  stage_mark(st, "k_narrow");
   const int* npairs = &d.ctr->n_pairs;
   scan_launch(d, d.pair_gcnt, d.pair_gstart, d.pair_cap, npairs, nullptr, st);
   scan_launch(d, d.pair_kept, d.pair_rstart, d.pair_cap, npairs, nullptr, st);
+  stage_mark(st, "scan_contact_offsets");
   k_emit<<<grid, 128, 0, st>>>(d, dims.dyn_row_cap, dims.dyn_group_cap);
+  stage_mark(st, "k_emit");
   scan_launch(d, d.dg_cnt, d.dg_start, d.nb, nullptr, nullptr, st);
+  stage_mark(st, "scan_incidence_offsets");
   k_dg_zero<<<grid, 256, 0, st>>>(d);
   k_dg_fill<<<grid, 256, 0, st>>>(d);
+  stage_mark(st, "k_dg_fill");
   k_dg_sort<<<grid, 128, 0, st>>>(d);
+  stage_mark(st, "k_dg_sort");
   g_kernel_launches += rebuild ? 13 : 12;  // the direct launches above (scans and sort count themselves)
 }
 

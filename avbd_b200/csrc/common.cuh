@@ -115,7 +115,7 @@ struct DevCounters {
   int n_cache_hits;      // warm-start cache hits in the last emission
   int n_new_contacts;    // cache misses in the last emission
   int max_dg;            // longest per-body dynamic incidence list
-  unsigned viol_bits[64];  // per-iteration max violation (float bits, >= 0)
+  unsigned viol_bits[AVBD_MAX_VIOL_ITERS];  // per-iteration max violation (float bits, >= 0)
   int n_viol;
   int n_marks;           // phase timestamps recorded (timing mode)
   int n_new_logged;      // new contacts queued for the learned warm start / log
@@ -138,8 +138,8 @@ struct DevCounters {
   int round_unc[2];  // uncolored counts of alternate coloring rounds
   int work_ctr[4];   // color passes: next chunk to hand out (pass q uses q & 3)
   int pad4[26];
-  unsigned vc_max_bits[64];  // per-iteration max violation over box-box contact groups (float bits)
-  int vc_cnt[64];            // and their count (record_violation)
+  unsigned vc_max_bits[AVBD_MAX_VIOL_ITERS];  // per-iteration max violation over box-box contact groups (float bits)
+  int vc_cnt[AVBD_MAX_VIOL_ITERS];            // and their count (record_violation)
 };
 #define BAR_SUB 16
 

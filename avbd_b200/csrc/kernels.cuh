@@ -8,6 +8,25 @@ namespace avbd {
 // per-substep launch count reported in the stats).
 extern thread_local long long g_kernel_launches;
 
+// Stage timing of one eager collision pipeline (avbd_profile_next_substep):
+// while a timer is installed on this thread, the launch functions record an
+// event after each stage.
+struct StageTimer {
+  static const int kMax = 48;
+  cudaEvent_t ev[kMax];
+  const char* name[kMax];
+  int n;
+};
+extern thread_local StageTimer* g_stage_timer;
+inline void stage_mark(cudaStream_t st, const char* name) {
+  StageTimer* t = g_stage_timer;
+  if (t && t->n < StageTimer::kMax) {
+    cudaEventRecord(t->ev[t->n], st);
+    t->name[t->n] = name;
+    t->n++;
+  }
+}
+
 void scan_launch(const Dev& d, const int* in, int* out, int n_cap, const int* n_dev, int* total_out,
                  cudaStream_t st);
 void radix_sort_launch(Dev& d, cudaStream_t st);
@@ -15,8 +34,14 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
 
 // Solve: coloring + predict + prelude + iterations + cache refresh.
 // persistent = one cooperative launch; otherwise one launch per phase.
+// With the flag-ordered sweep (P.flag_sweep) the persistent path is three
+// cooperative launches: head, the sweep (k_flag_sweep, `sweep_grid` CTAs),
+// tail.
 cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st,
-                         int variant);
+                         int variant, int sweep_grid);
+// CTAs of the standalone flag-sweep kernel for `group_size` lanes per body
+// (batched: the batched-scene instantiation) that fit on the GPU at once.
+int sweep_grid_size(int group_size, bool batched, int num_sms);
 // Resident CTAs per SM of the persistent kernel built for `variant` (2 or 3)
 // CTAs per SM.
 int solve_occupancy(int block, int variant);

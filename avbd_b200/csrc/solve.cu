@@ -714,7 +714,7 @@ __device__ __forceinline__ PassMode pass_mode(const DevParams& P, int it) {
   pm.post = P.post_stab && it == iters;
   pm.dual = it >= 1 && it <= iters;  // dual of iteration it-1
   pm.finalize = P.post_stab && it == iters && iters >= 1;
-  pm.viol_slot = (P.record_violation && pm.dual && it - 1 < 64 && !P.batched) ? it - 1 : -1;
+  pm.viol_slot = (P.record_violation && pm.dual && it - 1 < AVBD_MAX_VIOL_ITERS && !P.batched) ? it - 1 : -1;
   pm.it = it;
   return pm;
 }
@@ -1055,7 +1055,7 @@ __device__ void ph_dual(const Dev& d, int it, int gtid, int gsize) {
     d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
     d.g_flags[g] = fl;
   }
-  if (P.record_violation && it < 64) record_violation(d, it, vmax, csum, ccnt);
+  if (P.record_violation && it < AVBD_MAX_VIOL_ITERS) record_violation(d, it, vmax, csum, ccnt);
 }
 
 // Inertial target + warm start (kernels_6dof.py:122-187), plus the owner of
@@ -1537,17 +1537,21 @@ __device__ void ph_bucket_place(const Dev& d) {
 // Two register budgets of the same kernel: 2 CTAs/SM (128 registers) or
 // 3 CTAs/SM (80 registers); the host picks one (params.blocks_per_sm).
 
+// `mode`: 0 = the whole substep; 1 = the head (gate, prelude, coloring,
+// predict) only; 2 = the tail (last dual without post-stabilization,
+// collect) only.  Modes 1 and 2 bracket the flag-ordered sweep when it runs
+// as its own launch (k_flag_sweep), so the sweep gets a register budget of
+// its own.
 template <int MINB, bool BATCHED>
-__global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __grid_constant__ Dev d) {
+__global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __grid_constant__ Dev d, int mode) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   int gsize = gridDim.x * blockDim.x;
   int bar = 0;
   const DevParams& P = *d.prm;
   const bool timing = P.timing != 0;
   // SYNC(id): grid barrier; in timing mode thread 0 stamps the end of phase id.
-#define SYNC(id)                                                     \
+#define MARK(id)                                                     \
   do {                                                               \
-    if (!grid_barrier(d, bar++)) return;                             \
     if (timing && gtid == 0) {                                       \
       int m_ = d.ctr->n_marks;                                       \
       if (m_ < 256) {                                                \
@@ -1557,76 +1561,86 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
       }                                                              \
     }                                                                \
   } while (0)
-  if (timing && gtid == 0) {
-    d.ctr->mark_t[0] = gtimer();
-    d.ctr->mark_id[0] = PH_START;
-    d.ctr->n_marks = 1;
-  }
+#define SYNC(id)                                                     \
+  do {                                                               \
+    if (!grid_barrier(d, bar++)) return;                             \
+    MARK(id);                                                        \
+  } while (0)
   const bool jp = P.color_mode == 1;
   // Jones-Plassmann: the dataflow coloring runs alongside the gate and the
   // prelude, into color2, and is used only if the gate asks for new colors.
   const bool spec = jp && (long long)d.nb <= 32LL * gsize;
-  ph_gate(d, gtid, gsize);
-  ph_prelude<BATCHED>(d, gtid, gsize);  // reads x/q = the initial pose; predict runs after
-  ph_mlp_prelude(d, gtid, gsize);
-  if (spec) ph_color_dataflow(d, gtid, gsize);
-  SYNC(PH_GATE_PRELUDE);
-  if (recolor_needed(d)) {
-    if (spec) {
-      if (gtid == 0) d.ctr->recolored = 1;
-    } else {
-      ph_color_reset(d, gtid, gsize);
-      SYNC(PH_COLOR_RESET);
-    }
-    // Round r counts its uncolored bodies into round_unc[r & 1]; every block
-    // reads it after the round's last barrier.  The other slot is cleared
-    // during round r's second phase, when all blocks have read it.
-    int rounds = spec ? 0 : (jp ? JP_ROUNDS : MAX_COLORS);
-    for (int r = 0; r < rounds; ++r) {
-      int* unc_slot = &d.ctr->round_unc[r & 1];
-      ph_round_edges(d, jp, gtid, gsize);
-      SYNC(PH_ROUND);
-      if (gtid == 0) d.ctr->round_unc[(r + 1) & 1] = 0;
-      ph_round_assign(d, jp, unc_slot, gtid, gsize);
-      SYNC(PH_ROUND);
-      if (!jp) {
-        ph_resolve_edges(d, gtid, gsize);
-        SYNC(PH_ROUND);
-        ph_resolve_apply(d, unc_slot, gtid, gsize);
-        SYNC(PH_ROUND);
-      }
-      if (*(volatile int*)unc_slot == 0) break;
-    }
-    ph_bucket_count(d, spec);
-    SYNC(PH_BUCKET);
-    ph_bucket_scan(d);
-    SYNC(PH_BUCKET);
-    ph_bucket_place(d);
-  } else if (gtid == 0) {
-    d.ctr->recolored = 0;
-  }
-  ph_predict<BATCHED>(d, gtid, gsize);
-  SYNC(PH_PREDICT);
   int iters = P.iterations;
-  // batched scenes: one pass beyond the most iterations, where each scene
-  // runs its post-stab pass or its last dual + finalize
-  int total = iters + ((P.post_stab || P.batched) ? 1 : 0);
-  int nc = *(volatile int*)&d.ctr->n_colors;
-  // Pass `it` applies iteration it-1's dual update inside the color passes
-  // (owner-first), so each iteration is nc barriers; without a
-  // post-stabilization pass the last dual and the finalize run on their own.
-  if (P.flag_sweep && nc > 0) {
-    // all passes at once, each body ordered against its neighbours only
-    ph_flag_sweep<BATCHED>(d, total, nc, gtid, gsize);
-    SYNC(PH_PRIMAL);
-  } else {
-    for (int it = 0; it < total; ++it) {
-      PassMode pm = pass_mode(P, it);
-      for (int c = 0; c < nc; ++c) {
-        ph_primal<BATCHED>(d, c, pm, gtid, gsize, it * nc + c);
-        SYNC(PH_PRIMAL);
+  if (mode != 2) {
+    if (timing && gtid == 0) {
+      d.ctr->mark_t[0] = gtimer();
+      d.ctr->mark_id[0] = PH_START;
+      d.ctr->n_marks = 1;
+    }
+    ph_gate(d, gtid, gsize);
+    ph_prelude<BATCHED>(d, gtid, gsize);  // reads x/q = the initial pose; predict runs after
+    ph_mlp_prelude(d, gtid, gsize);
+    if (spec) ph_color_dataflow(d, gtid, gsize);
+    SYNC(PH_GATE_PRELUDE);
+    if (recolor_needed(d)) {
+      if (spec) {
+        if (gtid == 0) d.ctr->recolored = 1;
+      } else {
+        ph_color_reset(d, gtid, gsize);
+        SYNC(PH_COLOR_RESET);
+      }
+      // Round r counts its uncolored bodies into round_unc[r & 1]; every block
+      // reads it after the round's last barrier.  The other slot is cleared
+      // during round r's second phase, when all blocks have read it.
+      int rounds = spec ? 0 : (jp ? JP_ROUNDS : MAX_COLORS);
+      for (int r = 0; r < rounds; ++r) {
+        int* unc_slot = &d.ctr->round_unc[r & 1];
+        ph_round_edges(d, jp, gtid, gsize);
+        SYNC(PH_ROUND);
+        if (gtid == 0) d.ctr->round_unc[(r + 1) & 1] = 0;
+        ph_round_assign(d, jp, unc_slot, gtid, gsize);
+        SYNC(PH_ROUND);
+        if (!jp) {
+          ph_resolve_edges(d, gtid, gsize);
+          SYNC(PH_ROUND);
+          ph_resolve_apply(d, unc_slot, gtid, gsize);
+          SYNC(PH_ROUND);
+        }
+        if (*(volatile int*)unc_slot == 0) break;
+      }
+      ph_bucket_count(d, spec);
+      SYNC(PH_BUCKET);
+      ph_bucket_scan(d);
+      SYNC(PH_BUCKET);
+      ph_bucket_place(d);
+    } else if (gtid == 0) {
+      d.ctr->recolored = 0;
+    }
+    ph_predict<BATCHED>(d, gtid, gsize);
+    SYNC(PH_PREDICT);
+    if (mode == 1) return;
+    // batched scenes: one pass beyond the most iterations, where each scene
+    // runs its post-stab pass or its last dual + finalize
+    int total = iters + ((P.post_stab || P.batched) ? 1 : 0);
+    int nc = *(volatile int*)&d.ctr->n_colors;
+    // Pass `it` applies iteration it-1's dual update inside the color passes
+    // (owner-first), so each iteration is nc barriers; without a
+    // post-stabilization pass the last dual and the finalize run on their own.
+    if (P.flag_sweep && nc > 0) {
+      // all passes at once, each body ordered against its neighbours only
+      ph_flag_sweep<BATCHED>(d, total, nc, gtid, gsize);
+      SYNC(PH_PRIMAL);
+    } else {
+      for (int it = 0; it < total; ++it) {
+        PassMode pm = pass_mode(P, it);
+        for (int c = 0; c < nc; ++c) {
+          ph_primal<BATCHED>(d, c, pm, gtid, gsize, it * nc + c);
+          SYNC(PH_PRIMAL);
+        }
       }
     }
+  } else {
+    MARK(PH_PRIMAL);  // the sweep launch ended
   }
   if (!P.post_stab && !P.batched && iters >= 1) {
     ph_dual(d, iters - 1, gtid, gsize);
@@ -1639,9 +1653,27 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
   SYNC(PH_COLLECT);
   if (gtid == 0) {
     d.ctr->epoch += 1u;
-    d.ctr->n_viol = P.record_violation ? min(iters, 64) : 0;
+    d.ctr->n_viol = P.record_violation ? min(iters, AVBD_MAX_VIOL_ITERS) : 0;
   }
 #undef SYNC
+#undef MARK
+}
+
+// The flag-ordered sweep as a launch of its own, between the head and the
+// tail of the persistent kernel: G fixed at compile time and 20 warps per SM
+// (320 threads x 2 CTAs, 96 registers; inside the persistent kernel it runs
+// at 16 warps with every lane count's code in one register budget).  A
+// cooperative launch, so every CTA is resident: a warp's first chunk is
+// its index, and later chunks wait only on lower ones already running.
+#define SWEEP_BLOCK 320
+template <int G, bool B>
+__global__ void __launch_bounds__(SWEEP_BLOCK, 2) k_flag_sweep(const __grid_constant__ Dev d) {
+  int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  int gsize = gridDim.x * blockDim.x;
+  const DevParams& P = *d.prm;
+  int total = P.iterations + ((P.post_stab || P.batched) ? 1 : 0);
+  int nc = *(volatile int*)&d.ctr->n_colors;
+  if (nc > 0) flag_sweep<G, B>(d, total, nc, gtid, gsize);
 }
 
 // ---------------------------------------------------------------------------
@@ -1724,7 +1756,7 @@ __global__ void ks_collect(const __grid_constant__ Dev d) { GS; ph_collect(d, gt
 __global__ void ks_end(const __grid_constant__ Dev d) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     d.ctr->epoch += 1u;
-    d.ctr->n_viol = d.prm->record_violation ? min(d.prm->iterations, 64) : 0;
+    d.ctr->n_viol = d.prm->record_violation ? min(d.prm->iterations, AVBD_MAX_VIOL_ITERS) : 0;
   }
 }
 #undef GS
@@ -1745,19 +1777,50 @@ int solve_occupancy(int block, int variant) {
   return n;
 }
 
+static const void* sweep_kernel(int group_size, bool b) {
+  switch (group_size) {
+    case 1: return b ? (const void*)k_flag_sweep<1, true> : (const void*)k_flag_sweep<1, false>;
+    case 2: return b ? (const void*)k_flag_sweep<2, true> : (const void*)k_flag_sweep<2, false>;
+    case 4: return b ? (const void*)k_flag_sweep<4, true> : (const void*)k_flag_sweep<4, false>;
+    case 8: return b ? (const void*)k_flag_sweep<8, true> : (const void*)k_flag_sweep<8, false>;
+    case 16: return b ? (const void*)k_flag_sweep<16, true> : (const void*)k_flag_sweep<16, false>;
+    default: return b ? (const void*)k_flag_sweep<32, true> : (const void*)k_flag_sweep<32, false>;
+  }
+}
+
+int sweep_grid_size(int group_size, bool batched, int num_sms) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_kernel(group_size, batched), SWEEP_BLOCK, 0);
+  if (n > 2) n = 2;
+  return num_sms * (n > 0 ? n : 1);
+}
+
 cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st,
-                         int variant) {
+                         int variant, int sweep_grid) {
   // the bucket phases size their per-warp tables for this block size
   if (block != SOLVE_BLOCK) return cudaErrorInvalidConfiguration;
   // dynamic shared memory: the learned warm start's weights, when present
   size_t mlp_smem = d.mlp_w != nullptr ? sizeof(float) * AVBD_MLP_FLOATS : 0;
   if (persistent) {
-    void* args[] = {(void*)&d};
-    g_kernel_launches += 1;
     const bool b = d.n_scenes > 0;
     const void* fn = variant >= 3 ? (b ? (const void*)k_solve_persistent<3, true> : (const void*)k_solve_persistent<3, false>)
                                   : (b ? (const void*)k_solve_persistent<2, true> : (const void*)k_solve_persistent<2, false>);
-    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, mlp_smem, st);
+    if (!P.flag_sweep || sweep_grid <= 0) {
+      int mode = 0;
+      void* args[] = {(void*)&d, (void*)&mode};
+      g_kernel_launches += 1;
+      return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), args, mlp_smem, st);
+    }
+    int head = 1, tail = 2;
+    void* a_head[] = {(void*)&d, (void*)&head};
+    void* a_sweep[] = {(void*)&d};
+    void* a_tail[] = {(void*)&d, (void*)&tail};
+    g_kernel_launches += 3;
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), a_head, mlp_smem, st);
+    if (e != cudaSuccess) return e;
+    e = cudaLaunchCooperativeKernel(sweep_kernel(P.group_size, b), dim3(sweep_grid), dim3(SWEEP_BLOCK), a_sweep, 0, st);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), a_tail, mlp_smem, st);
   }
   ks_gate_prelude<<<grid, block, 0, st>>>(d);
   if (mlp_smem) {
@@ -1804,7 +1867,7 @@ __global__ void k_reset(const __grid_constant__ Dev d) {
     c->recolored = 0;
     c->bar_count = 0;
     for (int k = 0; k < BAR_SUB; ++k) c->bar_sub[k][0] = 0;
-    for (int k = 0; k < 64; ++k) {
+    for (int k = 0; k < AVBD_MAX_VIOL_ITERS; ++k) {
       c->viol_bits[k] = 0;
       c->vc_max_bits[k] = 0u;
       c->vc_cnt[k] = 0;

@@ -850,6 +850,21 @@ class Solver6DOF:
             out[name] = (ms + (t[k] - t[k - 1]) * 1e-6, cnt + 1)
         return out
 
+    @_on_stream
+    def collision_profile(self) -> dict:
+        """Runs one substep whose collision pipeline is launched eagerly with
+        a CUDA event after each stage, and returns {stage: device ms} (a scan
+        stage covers its three launches).  The substep is a real one: the
+        scene advances."""
+        self._flush()
+        L = _lib.load()
+        _lib.check(L.avbd_profile_next_substep(self._ctx), "profile")
+        self.substep()
+        cap = 48
+        ms = (C.c_float * cap)()
+        n = _lib.check(L.avbd_collision_profile(self._ctx, ms, cap), "collision profile")
+        return {L.avbd_collision_stage(self._ctx, k).decode(): float(ms[k]) for k in range(n)}
+
     def clear_errors(self) -> None:
         """Clear the sticky device error bits (after handling a reported error)."""
         if self._ctx is not None:

@@ -14,12 +14,12 @@ rows per contact: 50 seeds x 4 snapshots give about 2 M rows.  Training:
 the package's FP32 forward/backward kernels and Adam, 20 epochs.
 
 Evaluation on held-out seeds (1000..1009 by default; disjoint from
-training): for each snapshot, one substep of up to 64 iterations from three
-starts -- the plain zero start and the learned start, both with the cache
+training): for each snapshot, one substep of up to 256 iterations from
+three starts -- the plain zero start and the learned start, both with the cache
 emptied so every contact is new, and the full contact cache (the start the
-learned one stands in for: an upper bound).  Score: iterations until the max
-violation over all rows is <= 1e-4 m; the same over the box-box contact
-rows alone is reported beside it.
+learned one stands in for).  Score: iterations until the max violation over
+all rows is <= 1e-4 m (up to 256; 257 = not reached); the same over the
+box-box contact rows alone is reported beside it.
 
     python -m avbd_b200.train_warm_start
 """
@@ -67,7 +67,7 @@ def collect(seeds, size, frames, label_iterations=50):
     return np.concatenate(feats), np.concatenate(targs)
 
 
-def score_snapshot(s, iterations=64, tol=1e-4) -> dict:
+def score_snapshot(s, iterations=256, tol=1e-4) -> dict:
     """Iterations to `tol` max violation (all rows, and box-box contacts
     alone) from each of the three starts, at the solver's current state."""
     row = {}
@@ -81,7 +81,7 @@ def score_snapshot(s, iterations=64, tol=1e-4) -> dict:
     return row
 
 
-def evaluate(model, seeds, size, frames, iterations=64, tol=1e-4):
+def evaluate(model, seeds, size, frames, iterations=256, tol=1e-4):
     rows = []
     for seed in seeds:
         s = make_pile(seed, *size, model=model)

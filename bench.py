@@ -62,6 +62,74 @@ def algorithmic_bytes(n_bodies: int, r1: int, r2: int, n_pairs: int, pairs_with_
     return {"solve": solve, "collide": collide, "substep": solve + collide}
 
 
+def collision_stage_bytes(n: int, pairs: int, pairs_with: int, contacts: int) -> dict:
+    """Algorithmic bytes of each collision stage (what the stage must read
+    and write at least once; N bodies, P pairs, Pc pairs with contacts, K
+    contacts = dynamic groups, 2K incidences):
+      k_aabb       N x (pose 32 + half extents 16 + box out 32)           80 N
+      k_morton     N x (box 32 + code 4 + index 4)                        40 N
+      radix_sort   4 passes x N x (keys+indices in 8 + out 8 + hist 4)    80 N
+      k_lbvh_build (N-1) x (4 codes 16 + children/parent 16)             32 (N-1)
+      k_lbvh_leaves N x (box in 32 + leaf box out 32)                     64 N
+      k_lbvh_refit (N-1) x (2 child boxes 64 + box out 32)               96 (N-1)
+      k_lbvh_pack  (N-1) x (2 child boxes 64 + indices 8 + record 64)   136 (N-1)
+      k_bp_count   N x (own box 32 + count 4) + packed tree 64 (N-1)
+      k_bp_fill    as k_bp_count + pairs out 8 P
+      k_narrow     108 P + 140 Pc (two poses and extents, SAT / manifold out)
+      k_emit       K x (3 rows x 72 + cache probe 40)                    256 K
+      scans        12 B per scanned element (read twice, write once)
+      k_dg_fill    4 N (zero) + K x (bodies 8) + 2K x (entry 8)     4 N + 24 K
+      k_dg_sort    2K x (entry 8 read + 8 write)                          32 K"""
+    tree = 64 * max(n - 1, 0)
+    return {"k_aabb": 80 * n, "k_morton": 40 * n, "radix_sort": 80 * n, "k_lbvh_build": 32 * max(n - 1, 0),
+            "k_lbvh_leaves": 64 * n, "k_lbvh_refit": 96 * max(n - 1, 0), "k_lbvh_pack": 136 * max(n - 1, 0),
+            "k_bp_count": 36 * n + tree, "scan_pair_offsets": 12 * n, "k_bp_fill": 36 * n + tree + 8 * pairs,
+            "k_narrow": 108 * pairs + 140 * pairs_with, "scan_contact_offsets": 24 * pairs, "k_emit": 256 * contacts,
+            "scan_incidence_offsets": 12 * n, "k_dg_fill": 4 * n + 24 * contacts, "k_dg_sort": 32 * contacts}
+
+
+def collision_report(s, substeps: int = 8) -> dict:
+    """Per-stage device time (CUDA events between eager launches) over
+    `substeps` profiled substeps -- one LBVH rebuild and the refits between
+    -- with algorithmic GB/s from collision_stage_bytes."""
+    acc: dict = {}
+    for _ in range(substeps):
+        for k, v in s.collision_profile().items():
+            acc.setdefault(k, []).append(v)
+    st = s.stats()
+    p = s.pairs()
+    nb = len(s._x)
+    by = collision_stage_bytes(nb, int(st["n_pairs"]), int(np.sum(p["count"] > 0)), int(st["n_dyn_groups"]))
+    out = {}
+    for k, v in acc.items():
+        ms = float(np.mean(v))
+        row = {"ms": round(ms, 4), "runs_per_substep": round(len(v) / substeps, 3)}
+        if k in by and ms > 0:
+            row["gb_per_s"] = round(by[k] / (ms * 1e-3) / 1e9, 1)
+        out[k] = row
+    total = sum(r["ms"] * r["runs_per_substep"] for r in out.values())
+    return {"stages": out, "ms_per_substep": round(total, 4),
+            "note": "eager launches with an event after each stage (no graph); scans are three launches each"}
+
+
+def barrier_sweep_report(s) -> dict:
+    """Per-color pass time of the grid-barrier sweep (the option the flag
+    sweep replaces): one substep with phase stamps (globaltimer after each
+    grid barrier)."""
+    keep = (s.flag_sweep, s.timing)
+    s.flag_sweep, s.timing = False, True
+    try:
+        s.substep()
+        ph = s.phase_profile()
+        s.substep()
+        ph = s.phase_profile()
+    finally:
+        s.flag_sweep, s.timing = keep
+    ms, passes = ph.get("primal", (0.0, 0))
+    return {"passes": passes, "ms_per_pass": ms / max(1, passes), "primal_ms": ms,
+            "phases_ms": {k: round(v[0], 4) for k, v in ph.items()}}
+
+
 # ---------------------------------------------------------------------------
 # nvidia-smi clock sampler (runs during the timed region).
 # ---------------------------------------------------------------------------
@@ -248,36 +316,61 @@ def run_reference(args) -> None:
 # Second half of the metric: iterations to a violation tolerance, learned vs
 # plain (zero) warm start of new contacts.
 # ---------------------------------------------------------------------------
-def warm_start_eval(seeds=(1000, 1001), frames=(240, 400), iterations=64) -> dict:
-    """Held-out 16x16x8 piles (the training distribution; training used seeds
-    0-23) with the contact cache emptied, so every contact starts new; one
-    substep of up to 64 iterations from the plain zero start and from the
-    shipped learned start.  Scores: iterations until the max violation over
-    all rows <= 1e-4 m, and until the mean violation of the box-box contacts
-    <= 1e-5 m (65 = not reached)."""
-    from avbd_b200.learned import WarmStartMLP, cold_start_violation, iterations_to
-    from avbd_b200.train_warm_start import make_pile, snapshots
+def warm_start_eval(seeds=tuple(range(1000, 1010)), frames=(240, 400), iterations=256) -> dict:
+    """Held-out 16x16x8 piles of the benchmark distribution (the shipped
+    network was trained on seeds 0..49), at two snapshots each: one substep
+    of up to 256 iterations from the plain zero start and from the learned
+    start (both with the contact cache emptied, so every contact is new) and
+    from the full contact cache.  Score: iterations until the max violation
+    over all rows <= 1e-4 m (257 = not reached); the max over the box-box
+    contact rows alone beside it."""
+    from avbd_b200.learned import WarmStartMLP
+    from avbd_b200.train_warm_start import make_pile, score_snapshot, snapshots, summarize
     model = WarmStartMLP.load()
-    acc = {k: [] for k in ("plain_max", "learned_max", "plain_contact", "learned_contact")}
-    applied = new = 0
+    rows = []
     for seed in seeds:
         s = make_pile(seed, 16, 16, 8, model=model)
-        for _ in snapshots(s, frames):
-            for arm, learned in (("plain", False), ("learned", True)):
-                h, st = cold_start_violation(s, iterations, learned=learned)
-                acc[arm + "_max"].append(iterations_to(h, 1e-4))
-                acc[arm + "_contact"].append(iterations_to(st["contact_violation"], 1e-5))
-                if learned:
-                    applied += int(st["n_mlp_applied"])
-                    new += int(st["n_new_logged"])
-    m = {k: float(np.mean(v)) for k, v in acc.items()}
-    return {"workload": f"held-out 16x16x8 piles, seeds {list(seeds)}, frames {list(frames)}, contact cache emptied",
+        for f in snapshots(s, frames):
+            rows.append(dict(seed=seed, frame=f, **score_snapshot(s, iterations)))
+    d = summarize(rows)
+    return {"workload": (f"held-out 16x16x8 piles, seeds {seeds[0]}..{seeds[-1]}, frames {list(frames)}, one "
+                         "substep from each start"),
             "max_iterations": iterations,
-            "iters_to_1e-4m_max_violation": {"plain": m["plain_max"], "learned": m["learned_max"],
-                                              "reduction": 1.0 - m["learned_max"] / m["plain_max"]},
-            "iters_to_1e-5m_mean_contact_violation": {"plain": m["plain_contact"], "learned": m["learned_contact"],
-                                                      "reduction": 1.0 - m["learned_contact"] / m["plain_contact"]},
-            "learned_applied_fraction": applied / max(1, new)}
+            "iters_to_1e-4m_max_violation": {"plain": d["plain_max_iters"], "learned": d["learned_max_iters"],
+                                              "cached": d["cached_max_iters"],
+                                              "learned_reduction": d["learned_max_reduction"],
+                                              "cached_reduction": d["cached_max_reduction"]},
+            "iters_to_1e-4m_max_box_contact_violation": {"plain": d["plain_box_iters"],
+                                                          "learned": d["learned_box_iters"],
+                                                          "cached": d["cached_box_iters"]},
+            "learned_applied_fraction": d["applied_fraction"]}
+
+
+def warm_start_throughput(s, frames: int, warm: int = 3) -> dict:
+    """Body-substeps/s of the benchmark pile with the learned warm start on
+    and off (the network attached; `enabled` toggled), device time."""
+    import torch
+    from avbd_b200.learned import WarmStartMLP
+    model = WarmStartMLP.load()
+    s.warm_start = model
+    st = s._cuda_stream
+    nb = dyn_bodies(s)
+    out = {}
+    for arm, on in (("learned", True), ("plain", False)):
+        model.enabled = on
+        for _ in range(warm):
+            s.step()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st):
+            t0.record(st)
+        for _ in range(frames):
+            s._enqueue_step()
+        with torch.cuda.stream(st):
+            t1.record(st)
+        s._after_frame()
+        out[arm] = nb * PARAMS["substeps"] * frames / (t0.elapsed_time(t1) / 1e3)
+    s.warm_start = None
+    return {"body_substeps_per_s": out, "frames": frames, "learned_vs_plain": out["learned"] / out["plain"]}
 
 
 # ---------------------------------------------------------------------------
@@ -451,6 +544,8 @@ def run_gpu(args) -> None:
         "clocks": clk,
         "phase_ms_per_substep": {"collide": coll_ms, "solve": solve_ms},
     }
+    line["collision_kernels"] = collision_report(s)
+    line["barrier_sweep"] = barrier_sweep_report(s)
     if tuned is not None:
         line["autotune_ms_per_frame"] = {
             (f"G{r['group_size']}x{r['blocks_per_sm']}{'-flags' if r['flag_sweep'] else ''}"
@@ -464,6 +559,7 @@ def run_gpu(args) -> None:
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0 and not args.no_warm_start:
         line["warm_start"] = warm_start_eval()
+        line["warm_start"]["throughput_100k_pile"] = warm_start_throughput(s, frames=10)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

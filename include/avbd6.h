@@ -70,7 +70,7 @@ typedef struct AvbdDims {
 /* Scalars of Solver6DOF.__init__ (solver_6dof.py:180-201). */
 typedef struct AvbdParams {
   float dt; /* frame dt; a substep uses dt / substeps */
-  int iterations;
+  int iterations;     /* 0..256 (AVBD_MAX_VIOL_ITERS) */
   float gravity[3];
   float alpha, beta, gamma;
   int post_stabilize;
@@ -104,6 +104,9 @@ typedef struct AvbdParams {
                           the large colors */
 } AvbdParams;
 
+/* Iterations whose max violation a substep records (record_violation). */
+#define AVBD_MAX_VIOL_ITERS 256
+
 typedef struct AvbdStats {
   int n_pairs_found, n_pairs, n_dyn_groups, n_dyn_rows, n_dyn_rows_req;
   int n_contacts_req, n_colors, recolored, conflicts, err, err_where;
@@ -112,7 +115,7 @@ typedef struct AvbdStats {
   int graph_state;  /* bit 0: collision graph live, bit 1: solve graph live */
   int capture_err;  /* 1000 * collision capture error + solve capture error */
   long long kernels_launched; /* kernels enqueued by this context so far */
-  float viol[64];
+  float viol[AVBD_MAX_VIOL_ITERS];
   int n_new_logged;   /* new contacts queued last substep (may exceed new_cap) */
   int n_mlp_applied;  /* of those, warm-started by the MLP */
   int n_mlp_fallback; /* of those, kept at the zero start (separated, non-finite,
@@ -120,7 +123,7 @@ typedef struct AvbdStats {
   int n_mlp_reverted; /* learned starts reset to the zero start at their first
                          dual update because the contact separated (the
                          predicted force raised the complementarity residual) */
-  float viol_contact[64]; /* per-iteration max violation over box-box contacts */
+  float viol_contact[AVBD_MAX_VIOL_ITERS]; /* per-iteration max violation over box-box contacts */
 } AvbdStats;
 
 typedef struct AvbdCtx AvbdCtx;
@@ -182,6 +185,18 @@ int avbd_step_ms(AvbdCtx* ctx, float* collide_ms, float* solve_ms);
 /* Phase timestamps of the last substep's solve (params.timing = 1): up to
  * `cap` (globaltimer ns, phase id) pairs; returns the count.  Synchronises. */
 int avbd_read_phase_marks(AvbdCtx* ctx, long long* t_ns, int* phase, int cap, void* stream);
+
+/* Collision stage profile (no counterpart in the reference; it serves the
+ * per-kernel bandwidth report of the benchmark).  After
+ * avbd_profile_next_substep, the next substep launches its collision
+ * pipeline eagerly (no graph) with a CUDA event after each stage;
+ * avbd_collision_profile then writes up to `cap` stage durations in ms
+ * (synchronising on the last event) and returns their count;
+ * avbd_collision_stage names stage i ("k_aabb", "radix_sort", "k_bp_count",
+ * ..., a scan stage covers its three launches). */
+int avbd_profile_next_substep(AvbdCtx* ctx);
+int avbd_collision_profile(AvbdCtx* ctx, float* ms, int cap);
+const char* avbd_collision_stage(AvbdCtx* ctx, int i);
 
 /* Exclusive prefix sum of n int32 (out[0..n], out[n] = total) that allocates
  * no device memory.  No counterpart in the reference: it serves callers that
