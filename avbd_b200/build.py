@@ -24,6 +24,7 @@ UNITS = {
     "api.cu": [],
     "mlp.cu": [],
     "noalloc.cu": [],
+    "scene.cu": [],
 }
 
 

@@ -597,4 +597,17 @@ const char* avbd_collision_stage(AvbdCtx* c, int i) {
   return c->timer.name[i + 1];
 }
 
+int avbd_build_floor_groups(AvbdCtx* c, int nblk, const int* blk_body, const float* blk_he_fy,
+                            const float* blk_mat, const int* blk_row0, const int* blk_per, const int* blk_goff,
+                            void* stream) {
+  if (!c || nblk < 0 || (nblk > 0 && (!blk_body || !blk_he_fy || !blk_mat || !blk_row0 || !blk_per || !blk_goff)))
+    return fail(AVBD_E_INVALID, "bad floor-block arguments");
+  if (8LL * nblk > c->d.n_sg) return fail(AVBD_E_INVALID, "more floor corners than static groups");
+  if (nblk == 0) return AVBD_OK;
+  cudaError_t e = launch_floor_groups(c->d, nblk, blk_body, reinterpret_cast<const float4*>(blk_he_fy),
+                                      reinterpret_cast<const float4*>(blk_mat), blk_row0, blk_per, blk_goff,
+                                      (cudaStream_t)stream);
+  return e == cudaSuccess ? AVBD_OK : fail(AVBD_E_CUDA, "floor groups", e);
+}
+
 }  // extern "C"

@@ -46,6 +46,11 @@ int sweep_grid_size(int group_size, bool batched, int num_sms);
 // CTAs per SM.
 int solve_occupancy(int block, int variant);
 void launch_reset(Dev& d, cudaStream_t st);
+// Scene build: the 8 corner groups of each floor block at its group offset
+// (scene.cu).
+cudaError_t launch_floor_groups(const Dev& d, int nblk, const int* blk_body, const float4* blk_he_fy,
+                                const float4* blk_mat, const int* blk_row0, const int* blk_per, const int* blk_goff,
+                                cudaStream_t st);
 int count_conflicts(Dev& d, cudaStream_t st);
 void launch_hash_scrub(Dev& d, cudaStream_t st);
 void launch_cache_load(Dev& d, int n, const int* abc, const unsigned long long* keys, const float* st,

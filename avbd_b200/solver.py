@@ -15,6 +15,7 @@ extension missing, raises.
 from __future__ import annotations
 
 import ctypes as C
+import itertools
 import math
 import warnings
 from dataclasses import dataclass
@@ -112,6 +113,8 @@ class _RowTable:
         self._starts: list[int] = []  # first row of each segment
         self._segs: list = []  # list[_Row] (explicit rows) or a floor-block tuple
         self._n = 0
+        # the floor blocks again, column by column, for array construction
+        self._fb_cols: tuple = ([], [], [], [], [], [], [], [], [], [])  # body, hx, hy, hz, fy, mu, mus, stiff, start, per
 
     def __len__(self) -> int:
         return self._n
@@ -129,6 +132,8 @@ class _RowTable:
         per = 3 if mu > 0.0 else 1
         self._starts.append(start)
         self._segs.append((body, he, floor_y, mu, mus, stiffness, start, per))
+        for col, v in zip(self._fb_cols, (body, he[0], he[1], he[2], floor_y, mu, mus, stiffness, start, per)):
+            col.append(v)
         self._n += 8 * per
         return start
 
@@ -168,6 +173,18 @@ class _RowTable:
 
     def floor_blocks(self) -> list:
         return [seg for seg in self._segs if not isinstance(seg, list)]
+
+    def n_floor_blocks(self) -> int:
+        return len(self._fb_cols[0])
+
+    def floor_columns(self) -> dict:
+        """The floor blocks as arrays: body, he [n, 3], floor_y, mu, mus,
+        stiffness, first row, rows per corner."""
+        c = self._fb_cols
+        return dict(body=np.asarray(c[0], np.int64), he=np.stack([np.asarray(c[k], np.float64) for k in (1, 2, 3)], 1)
+                    if c[0] else np.zeros((0, 3)), fy=np.asarray(c[4], np.float32), mu=np.asarray(c[5], np.float32),
+                    mus=np.asarray(c[6], np.float32), stiff=np.asarray(c[7], np.float32),
+                    start=np.asarray(c[8], np.int64), per=np.asarray(c[9], np.int64))
 
 
 def box_inertia_local(mass: float, hx: float, hy: float, hz: float) -> np.ndarray:
@@ -327,6 +344,8 @@ class Solver6DOF:
         # explicit static groups (pins): (kind, body, row0, three, off, extra3, mu, mus, stiffness, fracture);
         # floor-contact groups live in the row table's floor blocks (8 each)
         self._groups: list[tuple] = []
+        self._layout = None
+        self._row_map_cache = None
         self._dirty = True
         self._self_collide = False
         self._self_friction = 0.0
@@ -363,12 +382,17 @@ class Solver6DOF:
     def add_box(self, position, half_extents, mass, orientation=(0.0, 0.0, 0.0, 1.0), velocity=(0.0, 0.0, 0.0),
                 angular_velocity=(0.0, 0.0, 0.0), friction=0.0) -> RigidBody:
         idx = len(self._x)
-        self._x.append(tuple(float(v) for v in position))
-        self._q.append(tuple(float(v) for v in orientation))
-        self._v.append(tuple(float(v) for v in velocity))
-        self._omega.append(tuple(float(v) for v in angular_velocity))
+        px, py, pz = position
+        qx, qy, qz, qw = orientation
+        vx, vy, vz = velocity
+        wx, wy, wz = angular_velocity
+        hx, hy, hz = half_extents
+        hx, hy, hz = float(hx), float(hy), float(hz)
+        self._x.append((float(px), float(py), float(pz)))
+        self._q.append((float(qx), float(qy), float(qz), float(qw)))
+        self._v.append((float(vx), float(vy), float(vz)))
+        self._omega.append((float(wx), float(wy), float(wz)))
         self._mass.append(float(mass))
-        hx, hy, hz = (float(h) for h in half_extents)
         self._half_extents.append((hx, hy, hz))
         self._friction.append(max(0.0, float(friction)))
         if self._scene_tab:
@@ -382,10 +406,11 @@ class Solver6DOF:
                               stiffness: float = _INF) -> list[int]:
         mu = float(friction) if friction is not None else self._friction[body.index]
         mus = mu * self.friction_static_mult if mu > 0.0 else 0.0
-        start = self._rows.add_floor_block(body.index, tuple(float(h) for h in body.half_extents), float(floor_y),
+        hx, hy, hz = body.half_extents
+        start = self._rows.add_floor_block(body.index, (float(hx), float(hy), float(hz)), float(floor_y),
                                            mu, mus, float(stiffness))
         per = 3 if mu > 0.0 else 1
-        out = [start + c * per for c in range(8)]
+        out = list(range(start, start + 8 * per, per))
         self._dirty = True
         return out
 
@@ -516,16 +541,18 @@ class Solver6DOF:
 
     @property
     def _n_static_groups(self) -> int:
-        return 8 * len(self._rows.floor_blocks()) + len(self._groups)
+        return 8 * self._rows.n_floor_blocks() + len(self._groups)
 
     def _static_group_arrays(self):
-        """Static groups sorted by body (stable: by first row within a body),
-        so each body's groups are one contiguous range; returns numpy arrays
-        and the static row -> (group, slot) map.  Floor corners are expanded
-        from their block records with array operations."""
+        """Host construction of the static groups, sorted by body (stable: by
+        first row within a body), so each body's groups are one contiguous
+        range; returns numpy arrays and the static row -> (group, slot) map.
+        The solver builds the same records on the device
+        (_upload_static_groups); this host form is what the tests compare
+        the device build with."""
         n = len(self._x)
-        fb = self._rows.floor_blocks()
-        nf = 8 * len(fb)
+        nblk = self._rows.n_floor_blocks()
+        nf = 8 * nblk
         ng = nf + len(self._groups)
         G = max(ng, 1)
         body = np.full((G, 2), -1, np.int32)
@@ -535,15 +562,10 @@ class Solver6DOF:
         gn = np.zeros((G, 4), np.float32)
         mat = np.zeros((G, 4), np.float32)
         three = np.zeros(G, bool)
-        if fb:
-            bb = np.array([f[0] for f in fb], np.int64)
-            he = np.array([f[1] for f in fb], np.float64)
-            fy = np.array([f[2] for f in fb], np.float32)
-            mu = np.array([f[3] for f in fb], np.float32)
-            mus = np.array([f[4] for f in fb], np.float32)
-            st = np.array([f[5] for f in fb], np.float32)
-            r0 = np.array([f[6] for f in fb], np.int64)
-            per = np.array([f[7] for f in fb], np.int64)
+        if nblk:
+            fc = self._rows.floor_columns()
+            bb, he, fy, mu, mus, st, r0, per = (fc[k] for k in ("body", "he", "fy", "mu", "mus", "stiff", "start",
+                                                                "per"))
             body[:nf, 0] = np.repeat(bb, 8)
             row0[:nf] = (r0[:, None] + np.arange(8)[None, :] * per[:, None]).reshape(-1)
             three[:nf] = np.repeat(per == 3, 8)
@@ -557,7 +579,7 @@ class Solver6DOF:
             body_he = np.asarray(self._half_extents, np.float32).reshape(-1, 3)[bb]
             imp = np.all(he.astype(np.float32) == body_he, axis=1)
             imp8 = np.repeat(imp, 8)
-            corner = np.tile(np.arange(8), len(fb))
+            corner = np.tile(np.arange(8), nblk)
             meta[:nf] |= np.where(imp8, META_IMPLICIT | (corner << 6), 0).astype(np.int32)
             explicit = (he[:, None, :] * _CORNER_SIGNS[None, :, :]).reshape(-1, 3).astype(np.float32)
             offa[:nf, :3] = np.where(imp8[:, None], 0.0, explicit)
@@ -597,6 +619,106 @@ class Solver6DOF:
         sg_start[1:] = np.cumsum(counts[:n])
         return out, sg_start, row_map
 
+    def _static_layout(self):
+        """Where each static group goes: floor blocks (8 corner groups each)
+        and explicit groups (pins) in one order, by body and then first row,
+        so a body's groups form one range.  Returns (floor-block columns,
+        first group of each block, group of each explicit group,
+        sg_start [n+1])."""
+        n = len(self._x)
+        fc = self._rows.floor_columns()
+        nblk = len(fc["body"])
+        ne = len(self._groups)
+        eb = np.fromiter((g[1] for g in self._groups), np.int64, ne)
+        er = np.fromiter((g[2] for g in self._groups), np.int64, ne)
+        body = np.concatenate([fc["body"], eb])
+        size = np.concatenate([np.full(nblk, 8, np.int64), np.ones(ne, np.int64)])
+        order = np.lexsort((np.concatenate([fc["start"], er]), body))
+        first = np.zeros(len(order), np.int64)
+        if len(order):
+            first[order] = np.concatenate([[0], np.cumsum(size[order])[:-1]])
+        counts = np.bincount(body, weights=size, minlength=n)[:n].astype(np.int64) if len(body) else np.zeros(n, np.int64)
+        sg_start = np.zeros(n + 1, np.int32)
+        sg_start[1:] = np.cumsum(counts)
+        return fc, first[:nblk], first[nblk:], sg_start
+
+    def _build_row_map(self) -> np.ndarray:
+        """Static row -> (group, row within the group) in the reference's row
+        numbering, from the static layout (computed when first needed)."""
+        fc, bfirst, efirst, _ = self._layout
+        rm = np.zeros((len(self._rows), 2), np.int64)
+        per = fc["per"]
+        if len(per):
+            nr = 8 * per
+            rel = np.arange(int(nr.sum())) - np.repeat(np.cumsum(nr) - nr, nr)
+            pr = np.repeat(per, nr)
+            rows = np.repeat(fc["start"], nr) + rel
+            rm[rows, 0] = np.repeat(bfirst, nr) + rel // pr
+            rm[rows, 1] = rel % pr
+        for j, g in enumerate(self._groups):
+            for s_ in range(3 if g[3] else 1):
+                rm[g[2] + s_] = (efirst[j], s_)
+        return rm
+
+    @property
+    def _row_map(self) -> np.ndarray:
+        if self._row_map_cache is None:
+            self._row_map_cache = self._build_row_map()
+        return self._row_map_cache
+
+    def _explicit_group_arrays(self, efirst):
+        """Records of the explicit static groups (pins) at their groups."""
+        ne = len(self._groups)
+        body = np.full((ne, 2), -1, np.int32)
+        meta = np.zeros(ne, np.int32)
+        row0 = np.zeros(ne, np.int32)
+        offa = np.zeros((ne, 4), np.float32)
+        gn = np.zeros((ne, 4), np.float32)
+        mat = np.zeros((ne, 4), np.float32)
+        flags = np.zeros(ne, np.int32)
+        for j, (kind, b, r0_, th, off, extra, mu_, mus_, stiff, frac) in enumerate(self._groups):
+            body[j, 0] = b
+            meta[j] = kind | (4 if th else 0) | (8 if not (stiff < _INF) else 0)
+            row0[j] = r0_
+            offa[j, :3] = off
+            if kind == KIND_FLOOR:
+                offa[j, 3] = extra[1]
+            else:
+                gn[j, :3] = extra
+            mat[j] = (mu_, mus_, stiff, frac)
+            flags[j] = 7 if th else 1
+        return dict(body=body, meta=meta, row0=row0, offa=offa, n=gn, mat=mat, flags=flags)
+
+    def _upload_static_groups(self) -> None:
+        """Static groups on the device: floor blocks expanded by
+        avbd_build_floor_groups (8 corner groups per block), explicit groups
+        (pins) written from host records, the per-body ranges (SG_START)."""
+        self._layout = fc, bfirst, efirst, sg_start = self._static_layout()
+        self._row_map_cache = None
+        dev = self.device
+        nblk = len(fc["body"])
+        if nblk:
+            i32 = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.int32)).to(dev)
+            he_fy = np.zeros((nblk, 4), np.float32)
+            he_fy[:, :3] = fc["he"]
+            he_fy[:, 3] = fc["fy"]
+            mat = np.zeros((nblk, 4), np.float32)
+            mat[:, 0], mat[:, 1], mat[:, 2] = fc["mu"], fc["mus"], fc["stiff"]
+            t = [i32(fc["body"]), torch.from_numpy(he_fy).to(dev), torch.from_numpy(mat).to(dev), i32(fc["start"]),
+                 i32(fc["per"]), i32(bfirst)]
+            _lib.check(_lib.load().avbd_build_floor_groups(self._ctx, nblk, *[C.c_void_p(x.data_ptr()) for x in t],
+                                                           self._stream()), "build floor groups")
+        if len(self._groups):
+            eg = self._explicit_group_arrays(efirst)
+            idx = torch.from_numpy(efirst).to(dev)
+            for name, arr in (("_g_body", eg["body"]), ("_g_meta", eg["meta"]), ("_g_row0", eg["row0"]),
+                              ("_g_offa", eg["offa"]), ("_g_n", eg["n"]), ("_g_mat", eg["mat"]),
+                              ("_g_flags", eg["flags"])):
+                getattr(self, name).index_copy_(0, idx, torch.from_numpy(arr).to(dev))
+            self._g_lam.index_fill_(0, idx, 0.0)
+            self._g_pen.index_fill_(0, idx, 1.0)  # solver_6dof.py:1121 (penalty seeded to 1)
+        self._sg_start.copy_(torch.from_numpy(sg_start))
+
     @_on_stream
     def _flush(self) -> None:
         if not self._dirty:
@@ -615,36 +737,27 @@ class Solver6DOF:
         self._views()
         dev = self.device
         if n:
-            m = np.array(self._mass, np.float32)
+            m = np.fromiter(self._mass, np.float32, n)
+            rows = lambda lst, k: np.fromiter(itertools.chain.from_iterable(lst), np.float32, k * n).reshape(n, k)
             x4 = np.zeros((n, 4), np.float32)
-            x4[:, :3] = np.array(self._x, np.float32)
+            x4[:, :3] = rows(self._x, 3)
             x4[:, 3] = m
             self.x4.copy_(torch.from_numpy(x4))
-            self.q.copy_(torch.from_numpy(np.array(self._q, np.float32).reshape(n, 4)))
-            self.v4[:, :3].copy_(torch.from_numpy(np.array(self._v, np.float32).reshape(n, 3)))
-            self.w4[:, :3].copy_(torch.from_numpy(np.array(self._omega, np.float32).reshape(n, 3)))
+            self.q.copy_(torch.from_numpy(rows(self._q, 4)))
+            self.v4[:, :3].copy_(torch.from_numpy(rows(self._v, 3)))
+            self.w4[:, :3].copy_(torch.from_numpy(rows(self._omega, 3)))
+            he = rows(self._half_extents, 3)
             he4 = np.zeros((n, 4), np.float32)
-            he4[:, :3] = np.array(self._half_extents, np.float32)
-            he4[:, 3] = np.array(self._friction, np.float32)
+            he4[:, :3] = he
+            he4[:, 3] = np.fromiter(self._friction, np.float32, n)
             self._he4.copy_(torch.from_numpy(he4))
             il = np.zeros((n, 4), np.float32)
-            il[:, :3] = _box_inertia_diag_batch(np.asarray(self._mass, np.float64),
-                                                np.asarray(self._half_extents, np.float64))
+            il[:, :3] = _box_inertia_diag_batch(np.fromiter(self._mass, np.float64, n),
+                                                np.fromiter(itertools.chain.from_iterable(self._half_extents),
+                                                            np.float64, 3 * n).reshape(n, 3))
             self._iloc4.copy_(torch.from_numpy(il))
             prio = np.random.default_rng(seed=0xA5BD).uniform(0.0, 1.0, size=n).astype(np.float32)
             self._prio.copy_(torch.from_numpy(prio))
-        sg, sg_start, self._row_map = self._static_group_arrays()
-        ng = self._n_static_groups
-        if ng:
-            self._g_body[:ng].copy_(torch.from_numpy(sg["body"][:ng]))
-            self._g_meta[:ng].copy_(torch.from_numpy(sg["meta"][:ng]))
-            self._g_row0[:ng].copy_(torch.from_numpy(sg["row0"][:ng]))
-            self._g_offa[:ng].copy_(torch.from_numpy(sg["offa"][:ng]))
-            self._g_n[:ng].copy_(torch.from_numpy(sg["n"][:ng]))
-            self._g_mat[:ng].copy_(torch.from_numpy(sg["mat"][:ng]))
-            self._g_flags[:ng].copy_(torch.from_numpy(sg["flags"][:ng]))
-            self._g_pen[:ng].fill_(1.0)  # solver_6dof.py:1121 (penalty seeded to 1)
-        self._sg_start.copy_(torch.from_numpy(sg_start))
         if prev is not None:
             k = prev[0]
             for dst, src in zip((self.x4, self.q, self.v4, self.w4, self.pv4, self.pw4), prev[1:]):
@@ -661,6 +774,7 @@ class Solver6DOF:
                    "create")
         self._ctx = ctx
         st = self._stream()
+        self._upload_static_groups()
         _lib.check(L.avbd_reset_state(self._ctx, st), "reset")
         self._pushed = None  # a new context starts without parameters
         self._push_params()

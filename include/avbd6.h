@@ -186,6 +186,19 @@ int avbd_step_ms(AvbdCtx* ctx, float* collide_ms, float* solve_ms);
  * `cap` (globaltimer ns, phase id) pairs; returns the count.  Synchronises. */
 int avbd_read_phase_marks(AvbdCtx* ctx, long long* t_ns, int* phase, int cap, void* stream);
 
+/* Scene build on the device (replaces the per-row loops of _flush,
+ * solver_6dof.py:1067-1129, for the rows of add_floor_contact_box,
+ * :474-541): writes the 8 corner groups of each of `nblk` floor blocks
+ * into the static group arrays of the arena.  Per block (device arrays):
+ * body; half extents and floor height (float4); mu, mu_s, stiffness
+ * (float4, 4th unused); first row number; rows per corner (3 with
+ * friction, else 1); first group index (blocks and explicit groups sorted
+ * by body, then first row).  Call after avbd_create, with the bodies' half
+ * extents (BHE) already in the arena. */
+int avbd_build_floor_groups(AvbdCtx* ctx, int nblk, const int* blk_body, const float* blk_he_fy,
+                            const float* blk_mat, const int* blk_row0, const int* blk_per, const int* blk_goff,
+                            void* stream);
+
 /* Collision stage profile (no counterpart in the reference; it serves the
  * per-kernel bandwidth report of the benchmark).  After
  * avbd_profile_next_substep, the next substep launches its collision
