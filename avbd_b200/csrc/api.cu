@@ -117,6 +117,18 @@ struct AvbdCtx {
   int graph_key[3][4];
   int capture_err[3];
   int part_kernels[3];
+  // Whole-frame graphs (avbd_step): the frame's substeps, each its
+  // collision part and solve part with event-record nodes between them, in
+  // one graph; one graph per pattern of LBVH rebuilds over the substeps.
+  static const int kFrameGraphs = 8;
+  cudaGraphExec_t fexec[kFrameGraphs];
+  cudaGraph_t fgraph[kFrameGraphs];
+  unsigned fpattern[kFrameGraphs];
+  int fkey[kFrameGraphs][16];
+  int fkernels[kFrameGraphs];
+  int nframe;
+  int frame_capture_err;
+  int frame_graph_used;  // the last avbd_step ran as one whole-frame graph
   int bvh_age;        // substeps since the last LBVH rebuild (0: none yet)
   int last_coll_part; // collision part of the last substep
   long long kernels_launched;
@@ -237,9 +249,20 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   return AVBD_OK;
 }
 
+static void drop_frame_graphs(AvbdCtx* c) {
+  for (int k = 0; k < c->nframe; ++k) {
+    if (c->fexec[k]) cudaGraphExecDestroy(c->fexec[k]);
+    if (c->fgraph[k]) cudaGraphDestroy(c->fgraph[k]);
+    c->fexec[k] = nullptr;
+    c->fgraph[k] = nullptr;
+  }
+  c->nframe = 0;
+}
+
 int avbd_destroy(AvbdCtx* c) {
   if (!c) return AVBD_OK;
   for (int part = 0; part < 3; ++part) drop_graph(c, part);
+  drop_frame_graphs(c);
   for (int k = 0; k < 3; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   for (int k = 0; k < StageTimer::kMax; ++k)
@@ -393,16 +416,22 @@ static cudaError_t run_part(AvbdCtx* c, int part, cudaStream_t st) {
   return e;
 }
 
+// Collision part of the next substep by the LBVH cadence (rebuild every
+// bvh_rebuild_every substeps, refit in between); advances the cadence.
+static int next_collision_part(AvbdCtx* c) {
+  bool collide = c->P.self_collide && c->d.nb >= 2;
+  int every = c->P.bvh_rebuild_every > 1 ? c->P.bvh_rebuild_every : 1;
+  bool rebuild = !collide || c->bvh_age == 0 || c->bvh_age >= every;
+  c->bvh_age = !collide ? 0 : (rebuild ? 1 : c->bvh_age + 1);
+  return rebuild ? 0 : 2;
+}
+
 static int run_substep(AvbdCtx* c, cudaStream_t st) {
   if (c->d.nb == 0) return AVBD_OK;
   if (c->substeps_done > 0 && c->substeps_done % 8192 == 0) launch_hash_scrub(c->d, st);
   // The pair list does not depend on the tree (pairs come out sorted by
   // body), so between rebuilds the LBVH is only refit to the new boxes.
-  bool collide = c->P.self_collide && c->d.nb >= 2;
-  int every = c->P.bvh_rebuild_every > 1 ? c->P.bvh_rebuild_every : 1;
-  bool rebuild = !collide || c->bvh_age == 0 || c->bvh_age >= every;
-  int part = rebuild ? 0 : 2;
-  c->bvh_age = !collide ? 0 : (rebuild ? 1 : c->bvh_age + 1);
+  int part = next_collision_part(c);
   c->last_coll_part = part;
   cudaEventRecord(c->ev[0], st);
   cudaError_t e;
@@ -448,7 +477,57 @@ int avbd_substep(AvbdCtx* c, float dt, void* stream) {
   if (!c) return fail(AVBD_E_INVALID, "null ctx");
   cudaStream_t st = (cudaStream_t)stream;
   int r = reset_slot(c, st);  // batched: one substep = slot 0, every scene at its own dt
+  c->frame_graph_used = 0;
   return r != AVBD_OK ? r : substep_impl(c, dt, st);
+}
+
+static void frame_key(AvbdCtx* c, unsigned pattern, int key[16]) {
+  std::memset(key, 0, 16 * sizeof(int));
+  part_key(c, 0, key);
+  part_key(c, 1, key + 4);
+  part_key(c, 2, key + 8);
+  key[12] = c->P.substeps;
+  key[13] = (int)pattern;
+}
+
+// Captures one frame: per substep, event ev[0], collision part, ev[1], solve
+// part, ev[2] (event-record nodes, so avbd_step_ms reads the last substep's
+// parts as with the per-part graphs).
+static int capture_frame(AvbdCtx* c, unsigned pattern, cudaStream_t st) {
+  if (c->nframe >= AvbdCtx::kFrameGraphs) drop_frame_graphs(c);
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    c->frame_capture_err = (int)e;
+    cudaGetLastError();
+    return -1;
+  }
+  long long before = g_kernel_launches;
+  cudaError_t le = cudaSuccess;
+  for (int s = 0; s < c->P.substeps && le == cudaSuccess; ++s) {
+    int part = ((pattern >> s) & 1u) ? 0 : 2;
+    le = cudaEventRecordWithFlags(c->ev[0], st, cudaEventRecordExternal);
+    if (le == cudaSuccess) le = enqueue_part(c, part, st);
+    if (le == cudaSuccess) le = cudaEventRecordWithFlags(c->ev[1], st, cudaEventRecordExternal);
+    if (le == cudaSuccess) le = enqueue_part(c, 1, st);
+    if (le == cudaSuccess) le = cudaEventRecordWithFlags(c->ev[2], st, cudaEventRecordExternal);
+  }
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(st, &g);
+  cudaGraphExec_t ex = nullptr;
+  if (le == cudaSuccess && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+    int k = c->nframe++;
+    c->fgraph[k] = g;
+    c->fexec[k] = ex;
+    c->fpattern[k] = pattern;
+    frame_key(c, pattern, c->fkey[k]);
+    c->fkernels[k] = (int)(g_kernel_launches - before);
+    cudaGetLastError();
+    return k;
+  }
+  c->frame_capture_err = (int)(le != cudaSuccess ? le : (e != cudaSuccess ? e : cudaErrorUnknown));
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  return -1;
 }
 
 int avbd_step(AvbdCtx* c, void* stream) {
@@ -456,6 +535,44 @@ int avbd_step(AvbdCtx* c, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   float dt = c->P.dt / (float)c->P.substeps;
   int r = reset_slot(c, st);
+  bool frame = c->P.use_graph && st != nullptr && c->d.nb > 0 && c->P.substeps <= 32 && !c->profile_next &&
+               c->frame_capture_err == 0;
+  if (r == AVBD_OK && frame) {
+    if (dt != c->cur_dt) {
+      c->cur_dt = dt;
+      fill_devparams(c, dt);
+      cudaError_t e = cudaMemcpyAsync((void*)c->d.prm, &c->dp, sizeof(DevParams), cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) return fail(AVBD_E_CUDA, "params upload", e);
+    }
+    // the contact-cache scrub, every 8192 substeps, runs before the frame it falls in
+    long long s0 = c->substeps_done;
+    for (int s = 0; s < c->P.substeps; ++s)
+      if (s0 + s > 0 && (s0 + s) % 8192 == 0) launch_hash_scrub(c->d, st);
+    int age0 = c->bvh_age;
+    unsigned pattern = 0;
+    int last = 0;
+    for (int s = 0; s < c->P.substeps; ++s) {
+      last = next_collision_part(c);
+      if (last == 0) pattern |= 1u << s;
+    }
+    int key[16];
+    frame_key(c, pattern, key);
+    int k = -1;
+    for (int j = 0; j < c->nframe; ++j)
+      if (std::memcmp(key, c->fkey[j], sizeof(key)) == 0) k = j;
+    if (k < 0) k = capture_frame(c, pattern, st);
+    if (k >= 0) {
+      cudaError_t e = cudaGraphLaunch(c->fexec[k], st);
+      if (e != cudaSuccess) return fail(AVBD_E_CUDA, "frame graph launch", e);
+      c->kernels_launched += c->fkernels[k];
+      c->substeps_done += c->P.substeps;
+      c->last_coll_part = last;
+      c->frame_graph_used = 1;
+      return settle_errors(AVBD_OK, "step");
+    }
+    c->bvh_age = age0;  // capture failed: the per-substep path below replays the cadence
+  }
+  c->frame_graph_used = 0;
   for (int s = 0; s < c->P.substeps && r == AVBD_OK; ++s) r = substep_impl(c, dt, st);
   return r;
 }
@@ -484,7 +601,7 @@ int avbd_read_stats(AvbdCtx* c, AvbdStats* out, void* stream) {
   out->max_dg = h.max_dg;
   out->n_viol = h.n_viol;
   out->epoch = h.epoch;
-  out->graph_state = (c->graph_ok[c->last_coll_part] ? 1 : 0) | (c->graph_ok[1] ? 2 : 0);
+  out->graph_state = c->frame_graph_used ? 7 : ((c->graph_ok[c->last_coll_part] ? 1 : 0) | (c->graph_ok[1] ? 2 : 0));
   out->capture_err = c->capture_err[c->last_coll_part] * 1000 + c->capture_err[1];
   out->kernels_launched = c->kernels_launched;
   out->n_new_logged = h.n_new_logged;

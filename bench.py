@@ -575,11 +575,12 @@ def run_gpu(args) -> None:
 def run_batched(args) -> None:
     """Batched scenes: 512 independent scenes (bodies log-uniform in
     [16, 2048], OBB heap distribution, per-scene friction, substeps in
-    {2, 4, 8}, iterations in {5, 10, 20}) stepped by one solver -- one
-    collision graph and one persistent solve launch per substep slot --
-    against launching the scenes one at a time (one Solver6DOF each, every
-    scene's frame enqueued back to back, one synchronisation per frame), on
-    the first `--seq-scenes` scenes for the ratio."""
+    {2, 4, 8}, iterations in {5, 10, 20}) stepped by one solver -- a frame
+    is one CUDA graph: every substep slot's collision launches and persistent
+    solve -- against launching the scenes one at a time (one Solver6DOF
+    each, every scene's frame enqueued back to back, one synchronisation per
+    frame), on the first `--seq-scenes` scenes (default all 512) for the
+    ratio."""
     import torch
     import torch.distributed as dist
     from avbd_b200.autotune import autotune
@@ -706,7 +707,7 @@ def main():
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start evaluation")
     ap.add_argument("--row-capacity", type=int, default=0, help="initial dynamic-row pool (0 = reference size)")
     ap.add_argument("--batched", action="store_true", help="512 batched scenes vs one scene at a time")
-    ap.add_argument("--seq-scenes", type=int, default=64, help="scenes in the one-at-a-time comparison")
+    ap.add_argument("--seq-scenes", type=int, default=512, help="scenes in the one-at-a-time comparison")
     ap.add_argument("--settle-batched", type=int, default=60)
     args = ap.parse_args()
     if args.warmup < 3:

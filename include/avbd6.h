@@ -112,7 +112,9 @@ typedef struct AvbdStats {
   int n_contacts_req, n_colors, recolored, conflicts, err, err_where;
   int n_cache_hits, n_new_contacts, max_dg, n_viol;
   unsigned epoch;
-  int graph_state;  /* bit 0: collision graph live, bit 1: solve graph live */
+  int graph_state;  /* bit 0: collision graph live, bit 1: solve graph live,
+                       bit 2: the last avbd_step ran as one whole-frame graph
+                       (all substeps, collision and solve; bits 0-1 set too) */
   int capture_err;  /* 1000 * collision capture error + solve capture error */
   long long kernels_launched; /* kernels enqueued by this context so far */
   float viol[AVBD_MAX_VIOL_ITERS];

@@ -31,7 +31,7 @@ def test_refit_tree_gives_the_rebuilt_trajectory(every):
     np.testing.assert_array_equal(a.positions(), b.positions())
     np.testing.assert_array_equal(a.orientations(), b.orientations())
     st = b.stats()
-    assert st["err"] == 0 and st["graph_state"] == 3
+    assert st["err"] == 0 and st["graph_state"] == 7  # each frame one whole-frame graph
 
 
 def test_refit_after_teleport():

@@ -132,7 +132,29 @@ def test_graph_and_direct_launch_bit_identical():
         a.step()
         b.step()
     np.testing.assert_array_equal(a.positions(), b.positions())
-    assert a.stats()["graph_state"] == 3
+    assert a.stats()["graph_state"] == 7  # step(): all substeps in one whole-frame graph
+
+
+def test_frame_graph_equals_substep_graphs():
+    """step() replays one graph per frame (every substep's collision and
+    solve, the LBVH rebuild cadence baked into per-pattern graphs);
+    substep() replays the per-part graphs.  Same results bit for bit, and the
+    event-record nodes inside the frame graph still time the last substep's
+    collision and solve."""
+    build, params = CASES["pile-pins-jp"]
+    a = make_gpu(**params)
+    b = make_gpu(**params)
+    a.bvh_rebuild_every = b.bvh_rebuild_every = 3  # rebuilds at different substeps of different frames
+    build(a)
+    build(b)
+    for _ in range(7):
+        a.step()
+        for _ in range(params["substeps"]):
+            b.substep()
+    np.testing.assert_array_equal(a.positions(), b.positions())
+    np.testing.assert_array_equal(a.orientations(), b.orientations())
+    assert a.stats()["graph_state"] == 7 and b.stats()["graph_state"] == 3
+    assert a.broadphase_ms > 0.0 and a.solve_ms > 0.0
 
 
 def test_long_run_statistics_match():
