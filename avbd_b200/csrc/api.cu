@@ -435,14 +435,26 @@ static int run_substep(AvbdCtx* c, cudaStream_t st) {
   c->last_coll_part = part;
   cudaEventRecord(c->ev[0], st);
   cudaError_t e;
-  if (c->profile_next) {  // eager launches with a stage event after each
+  if (c->profile_next) {  // a one-off graph of the pipeline with an event node after each stage
     c->timer.n = 0;
-    g_stage_timer = &c->timer;
-    e = enqueue_part(c, part, st);
-    g_stage_timer = nullptr;
-    c->kernels_launched += c->part_kernels[part];
     c->profile_next = 0;
-    c->profile_ready = 1;
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      g_stage_timer = &c->timer;
+      cudaError_t le = enqueue_part(c, part, st);
+      g_stage_timer = nullptr;
+      cudaGraph_t g = nullptr;
+      e = cudaStreamEndCapture(st, &g);
+      if (le != cudaSuccess) e = le;
+      cudaGraphExec_t ex = nullptr;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+      if (e == cudaSuccess) e = cudaGraphLaunch(ex, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (ex) cudaGraphExecDestroy(ex);
+      if (g) cudaGraphDestroy(g);
+    }
+    c->kernels_launched += c->part_kernels[part];
+    c->profile_ready = e == cudaSuccess;
   } else {
     e = run_part(c, part, st);
   }
@@ -694,6 +706,7 @@ int avbd_profile_next_substep(AvbdCtx* c) {
 }
 
 int avbd_collision_profile(AvbdCtx* c, float* ms, int cap) {
+  // (the profiled pipeline ran as a one-off graph; its events are complete)
   if (!c || (!ms && cap > 0)) return fail(AVBD_E_INVALID, "null argument");
   if (!c->profile_ready) return fail(AVBD_E_INVALID, "no profiled substep has run");
   int n = c->timer.n;

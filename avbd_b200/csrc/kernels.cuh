@@ -8,9 +8,10 @@ namespace avbd {
 // per-substep launch count reported in the stats).
 extern thread_local long long g_kernel_launches;
 
-// Stage timing of one eager collision pipeline (avbd_profile_next_substep):
-// while a timer is installed on this thread, the launch functions record an
-// event after each stage.
+// Stage timing of one collision pipeline (avbd_profile_next_substep): while
+// a timer is installed on this thread, the launch functions record an event
+// after each stage (captured into a one-off graph, so no host launch gaps
+// sit between the stages).
 struct StageTimer {
   static const int kMax = 48;
   cudaEvent_t ev[kMax];
@@ -21,7 +22,8 @@ extern thread_local StageTimer* g_stage_timer;
 inline void stage_mark(cudaStream_t st, const char* name) {
   StageTimer* t = g_stage_timer;
   if (t && t->n < StageTimer::kMax) {
-    cudaEventRecord(t->ev[t->n], st);
+    // an event-record node when the pipeline is being captured
+    cudaEventRecordWithFlags(t->ev[t->n], st, cudaEventRecordExternal);
     t->name[t->n] = name;
     t->n++;
   }

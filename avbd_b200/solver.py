@@ -966,8 +966,8 @@ class Solver6DOF:
 
     @_on_stream
     def collision_profile(self) -> dict:
-        """Runs one substep whose collision pipeline is launched eagerly with
-        a CUDA event after each stage, and returns {stage: device ms} (a scan
+        """Runs one substep whose collision pipeline replays as a one-off
+        graph with an event after each stage, and returns {stage: device ms} (a scan
         stage covers its three launches).  The substep is a real one: the
         scene advances."""
         self._flush()

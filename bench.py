@@ -89,7 +89,8 @@ def collision_stage_bytes(n: int, pairs: int, pairs_with: int, contacts: int) ->
 
 
 def collision_report(s, substeps: int = 8) -> dict:
-    """Per-stage device time (CUDA events between eager launches) over
+    """Per-stage device time (event-record nodes between the stages of a
+    one-off graph of the pipeline) over
     `substeps` profiled substeps -- one LBVH rebuild and the refits between
     -- with algorithmic GB/s from collision_stage_bytes."""
     acc: dict = {}
@@ -109,7 +110,7 @@ def collision_report(s, substeps: int = 8) -> dict:
         out[k] = row
     total = sum(r["ms"] * r["runs_per_substep"] for r in out.values())
     return {"stages": out, "ms_per_substep": round(total, 4),
-            "note": "eager launches with an event after each stage (no graph); scans are three launches each"}
+            "note": "one-off graph of the pipeline with an event-record node after each stage; scans are three launches each"}
 
 
 def barrier_sweep_report(s) -> dict:

@@ -203,10 +203,10 @@ int avbd_build_floor_groups(AvbdCtx* ctx, int nblk, const int* blk_body, const f
 
 /* Collision stage profile (no counterpart in the reference; it serves the
  * per-kernel bandwidth report of the benchmark).  After
- * avbd_profile_next_substep, the next substep launches its collision
- * pipeline eagerly (no graph) with a CUDA event after each stage;
- * avbd_collision_profile then writes up to `cap` stage durations in ms
- * (synchronising on the last event) and returns their count;
+ * avbd_profile_next_substep, the next substep runs its collision pipeline
+ * as a one-off CUDA graph with an event-record node after each stage (and
+ * synchronises); avbd_collision_profile then writes up to `cap` stage
+ * durations in ms and returns their count;
  * avbd_collision_stage names stage i ("k_aabb", "radix_sort", "k_bp_count",
  * ..., a scan stage covers its three launches). */
 int avbd_profile_next_substep(AvbdCtx* ctx);
