@@ -109,6 +109,7 @@ struct AvbdCtx {
   int coll_grid;
   int solve_grid, solve_block, solve_variant;
   int sweep_grid;  // CTAs of the standalone flag-sweep launch (0: the sweep runs inside the persistent kernel)
+  int sweep_minb;  // CTAs per SM the sweep launch is built for (2: 320 threads, 3: 256 threads)
   // parts: 0 = collision with an LBVH rebuild, 1 = solve, 2 = collision
   // that refits the previous tree
   cudaGraphExec_t exec[3];
@@ -317,12 +318,17 @@ int avbd_set_params(AvbdCtx* c, const AvbdParams* p, void* stream) {
   if (e != cudaSuccess) return fail(AVBD_E_CUDA, "params upload", e);
   // Persistent grid: `blocks_per_sm` CTAs per SM (0 = 2), using the
   // register budget built for it, capped by the measured occupancy.
+  // With the flag sweep as its own launch, blocks_per_sm shapes that launch;
+  // the persistent head and tail keep the 2-CTA build (the 3-CTA build
+  // spills 2.8 KB per thread).
   int want = p->blocks_per_sm > 0 ? p->blocks_per_sm : 2;
+  c->sweep_minb = want >= 3 ? 3 : 2;
+  if (p->flag_sweep) want = 2;
   c->solve_variant = want >= 3 ? 3 : 2;
   int occ = solve_occupancy(256, c->solve_variant);
   int b = want < occ ? want : occ;
   c->solve_grid = c->num_sms * (b > 0 ? b : 1);
-  c->sweep_grid = p->flag_sweep ? sweep_grid_size(p->group_size, c->d.n_scenes > 0, c->num_sms) : 0;
+  c->sweep_grid = p->flag_sweep ? sweep_grid_size(p->group_size, c->d.n_scenes > 0, c->num_sms, c->sweep_minb) : 0;
   return AVBD_OK;
 }
 
@@ -351,7 +357,7 @@ static cudaError_t enqueue_part(AvbdCtx* c, int part, cudaStream_t st) {
     e = cudaGetLastError();
   } else {
     e = launch_solve(c->d, c->P, c->P.persistent, c->solve_grid, c->solve_block, st, c->solve_variant,
-                     c->sweep_grid);
+                     c->sweep_grid, c->sweep_minb);
   }
   c->part_kernels[part] = (int)(g_kernel_launches - before);
   return e;

@@ -40,10 +40,11 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
 // cooperative launches: head, the sweep (k_flag_sweep, `sweep_grid` CTAs),
 // tail.
 cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st,
-                         int variant, int sweep_grid);
+                         int variant, int sweep_grid, int sweep_minb);
 // CTAs of the standalone flag-sweep kernel for `group_size` lanes per body
-// (batched: the batched-scene instantiation) that fit on the GPU at once.
-int sweep_grid_size(int group_size, bool batched, int num_sms);
+// (batched: the batched-scene instantiation) built for `blocks_per_sm` (2 or
+// 3) CTAs per SM that fit on the GPU at once.
+int sweep_grid_size(int group_size, bool batched, int num_sms, int blocks_per_sm);
 // Resident CTAs per SM of the persistent kernel built for `variant` (2 or 3)
 // CTAs per SM.
 int solve_occupancy(int block, int variant);

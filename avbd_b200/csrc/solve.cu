@@ -1662,12 +1662,13 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, MINB) k_solve_persistent(const __
 // The flag-ordered sweep as a launch of its own, between the head and the
 // tail of the persistent kernel: G fixed at compile time and 20 warps per SM
 // (320 threads x 2 CTAs, 96 registers; inside the persistent kernel it runs
-// at 16 warps with every lane count's code in one register budget).  A
+// at 16 warps with every lane count's code in one register budget), or 24
+// warps per SM (256 threads x 3 CTAs, 80 registers, more spills).  A
 // cooperative launch, so every CTA is resident: a warp's first chunk is
 // its index, and later chunks wait only on lower ones already running.
-#define SWEEP_BLOCK 320
-template <int G, bool B>
-__global__ void __launch_bounds__(SWEEP_BLOCK, 2) k_flag_sweep(const __grid_constant__ Dev d) {
+#define SWEEP_BLOCK_FOR(minb) ((minb) >= 3 ? 256 : 320)
+template <int G, bool B, int MINB>
+__global__ void __launch_bounds__(SWEEP_BLOCK_FOR(MINB), MINB) k_flag_sweep(const __grid_constant__ Dev d) {
   int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   int gsize = gridDim.x * blockDim.x;
   const DevParams& P = *d.prm;
@@ -1777,26 +1778,33 @@ int solve_occupancy(int block, int variant) {
   return n;
 }
 
-static const void* sweep_kernel(int group_size, bool b) {
+template <int MINB>
+static const void* sweep_kernel_m(int group_size, bool b) {
   switch (group_size) {
-    case 1: return b ? (const void*)k_flag_sweep<1, true> : (const void*)k_flag_sweep<1, false>;
-    case 2: return b ? (const void*)k_flag_sweep<2, true> : (const void*)k_flag_sweep<2, false>;
-    case 4: return b ? (const void*)k_flag_sweep<4, true> : (const void*)k_flag_sweep<4, false>;
-    case 8: return b ? (const void*)k_flag_sweep<8, true> : (const void*)k_flag_sweep<8, false>;
-    case 16: return b ? (const void*)k_flag_sweep<16, true> : (const void*)k_flag_sweep<16, false>;
-    default: return b ? (const void*)k_flag_sweep<32, true> : (const void*)k_flag_sweep<32, false>;
+    case 1: return b ? (const void*)k_flag_sweep<1, true, MINB> : (const void*)k_flag_sweep<1, false, MINB>;
+    case 2: return b ? (const void*)k_flag_sweep<2, true, MINB> : (const void*)k_flag_sweep<2, false, MINB>;
+    case 4: return b ? (const void*)k_flag_sweep<4, true, MINB> : (const void*)k_flag_sweep<4, false, MINB>;
+    case 8: return b ? (const void*)k_flag_sweep<8, true, MINB> : (const void*)k_flag_sweep<8, false, MINB>;
+    case 16: return b ? (const void*)k_flag_sweep<16, true, MINB> : (const void*)k_flag_sweep<16, false, MINB>;
+    default: return b ? (const void*)k_flag_sweep<32, true, MINB> : (const void*)k_flag_sweep<32, false, MINB>;
   }
 }
+static const void* sweep_kernel(int group_size, bool b, int minb) {
+  return minb >= 3 ? sweep_kernel_m<3>(group_size, b) : sweep_kernel_m<2>(group_size, b);
+}
 
-int sweep_grid_size(int group_size, bool batched, int num_sms) {
+int sweep_block_size(int blocks_per_sm) { return SWEEP_BLOCK_FOR(blocks_per_sm); }
+
+int sweep_grid_size(int group_size, bool batched, int num_sms, int blocks_per_sm) {
+  int minb = blocks_per_sm >= 3 ? 3 : 2;
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_kernel(group_size, batched), SWEEP_BLOCK, 0);
-  if (n > 2) n = 2;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_kernel(group_size, batched, minb), SWEEP_BLOCK_FOR(minb), 0);
+  if (n > minb) n = minb;
   return num_sms * (n > 0 ? n : 1);
 }
 
 cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, int block, cudaStream_t st,
-                         int variant, int sweep_grid) {
+                         int variant, int sweep_grid, int sweep_minb) {
   // the bucket phases size their per-warp tables for this block size
   if (block != SOLVE_BLOCK) return cudaErrorInvalidConfiguration;
   // dynamic shared memory: the learned warm start's weights, when present
@@ -1818,7 +1826,8 @@ cudaError_t launch_solve(Dev& d, const AvbdParams& P, int persistent, int grid, 
     g_kernel_launches += 3;
     cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), a_head, mlp_smem, st);
     if (e != cudaSuccess) return e;
-    e = cudaLaunchCooperativeKernel(sweep_kernel(P.group_size, b), dim3(sweep_grid), dim3(SWEEP_BLOCK), a_sweep, 0, st);
+    e = cudaLaunchCooperativeKernel(sweep_kernel(P.group_size, b, sweep_minb), dim3(sweep_grid),
+                                    dim3(SWEEP_BLOCK_FOR(sweep_minb)), a_sweep, 0, st);
     if (e != cudaSuccess) return e;
     return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(block), a_tail, mlp_smem, st);
   }

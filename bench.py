@@ -541,7 +541,7 @@ def run_gpu(args) -> None:
                                     "autotuned": tuned is not None},
                    "scene_build_s": {"total": round(t_build, 3), "api_calls": round(t_api, 3),
                                      "flush": round(t_flush, 3)}},
-        "roofline": {"bound": "hbm", "kernel": "k_solve_persistent", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "solve (k_solve_persistent head + k_flag_sweep + tail)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": ab["solve"], "launch_ms": solve_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
