@@ -46,9 +46,12 @@ def _time_frames(solver, frames: int, warm: int) -> float:
 
 
 def autotune(solver, group_sizes=(4, 8, 16), blocks_per_sm=(2, 3), flag_sweep=(False, True),
-             adaptive_lanes=(False, True), frames: int = 2, warm: int = 1, apply: bool = True) -> dict:
+             adaptive_lanes=(False, True), frames: int = 2, warm: int = 2, apply: bool = True) -> dict:
     """Times each (group size, CTAs per SM, sweep ordering, adaptive lanes)
-    candidate for `frames` frames and returns {"best": {...}, "table":
+    candidate for `frames` frames (after `warm` untimed frames: a frame is
+    one CUDA graph per LBVH rebuild pattern, and consecutive frames can
+    differ in pattern, so two warm frames capture both before timing) and
+    returns {"best": {...}, "table":
     [...]}; sets the best candidate on the solver when `apply`.  Adaptive
     lanes only apply to the barrier sweep, so flag-sweep candidates are timed
     without them.  The scene state is restored afterwards."""
