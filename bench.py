@@ -374,6 +374,76 @@ def warm_start_throughput(s, frames: int, warm: int = 3) -> dict:
     return {"body_substeps_per_s": out, "frames": frames, "learned_vs_plain": out["learned"] / out["plain"]}
 
 
+def batched_summary(frames: int = 5, seq_frames: int = 3, settle: int = 60) -> dict:
+    """The batched-scenes comparison in a form short enough for the main
+    bench line: the 512 scenes batched (one CUDA graph per frame, lanes per
+    body 4 with the flag sweep), and the same 512 scenes as 512 Solver6DOF
+    stepped one at a time.  The single solvers start from the batch's
+    settled bodies (positions, orientations, velocities copied per scene,
+    so the 512 of them need not settle again); each runs 4 untimed frames
+    (contacts, cache and coloring rebuild, and every LBVH rebuild pattern's
+    frame graph is captured) before its timed ones."""
+    import torch
+    from avbd_b200.batch import c4_batch, c4_single, c4_specs
+    specs = c4_specs(512, seed=0)
+    b = c4_batch(specs)
+    b.solver.primal_group_size = 4
+    for _ in range(settle):
+        b.solver._enqueue_step()
+    b.solver._after_frame()
+    for _ in range(2):
+        b.step()
+    st = b.solver._cuda_stream
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        t0.record(st)
+    for _ in range(frames):
+        b.solver._enqueue_step()
+    with torch.cuda.stream(st):
+        t1.record(st)
+    b.solver._after_frame()
+    ms_b = t0.elapsed_time(t1) / frames
+    value_b = b.body_substeps_per_frame() / (ms_b * 1e-3)
+    x, q, v, w = b.solver.x4, b.solver.q, b.solver.v4, b.solver.w4
+    singles = []
+    for sc, spec in zip(b.scenes, specs):
+        s1 = c4_single(spec)
+        s1._flush()
+        idx = torch.as_tensor([bd.index for bd in sc.bodies], device=x.device)
+        org = torch.as_tensor(np.append(sc.origin, 0.0), dtype=torch.float32, device=x.device)
+        with torch.cuda.stream(s1._cuda_stream):
+            s1.x4[: len(idx)].copy_(x[idx] - org)
+            s1.q[: len(idx)].copy_(q[idx])
+            s1.v4[: len(idx)].copy_(v[idx])
+            s1.w4[: len(idx)].copy_(w[idx])
+        singles.append(s1)
+    torch.cuda.synchronize()
+    for _ in range(4):
+        for s1 in singles:
+            s1._enqueue_step()
+        for s1 in singles:
+            s1._after_frame()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(seq_frames):
+        for s1 in singles:
+            s1._enqueue_step()
+        for s1 in singles:
+            s1._cuda_stream.synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_s = e0.elapsed_time(e1) / seq_frames
+    units = sum(sum(1 for m in s1._mass if m > 0) * s1.substeps for s1 in singles)
+    value_s = units / (ms_s * 1e-3)
+    return {"workload": ("512 scenes, bodies log-uniform [16, 2048] (OBB heaps with 4 walls), substeps {2,4,8}, "
+                         f"iterations {{5,10,20}}, settled {settle} frames; batched: one CUDA graph per frame; "
+                         "one at a time: 512 Solver6DOF, one frame graph each, frames enqueued back to back"),
+            "batched": {"value": value_b, "ms_per_frame": ms_b},
+            "one_at_a_time": {"value": value_s, "ms_per_frame": ms_s},
+            "speedup": value_b / value_s, "unit": UNIT}
+
+
 # ---------------------------------------------------------------------------
 # Multi-GPU: replicas only.  Each rank runs its own pile; the only collective
 # is this max of the per-rank timings (the job is as fast as its slowest rank).
@@ -563,6 +633,8 @@ def run_gpu(args) -> None:
         # the oracle), a few substeps: the same configuration as `value`
         cb = port_full_rate(s.state_dict(), substeps=3, warmup=1, threads=threads, size=size, settle=args.settle)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0 and world == 1 and not args.no_batched:
+        line["batched_scenes_512"] = batched_summary()
     if rank == 0 and not args.no_warm_start:
         line["warm_start"] = warm_start_eval()
         line["warm_start"]["throughput_100k_pile"] = warm_start_throughput(s, frames=10)
@@ -706,6 +778,7 @@ def main():
                          "times Solver6DOF's own default shape, as a drop-in user gets it)")
     ap.add_argument("--no-tune", action="store_true", help="batched bench: skip the autotuner")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start evaluation")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 512-scene batched comparison key")
     ap.add_argument("--row-capacity", type=int, default=0, help="initial dynamic-row pool (0 = reference size)")
     ap.add_argument("--batched", action="store_true", help="512 batched scenes vs one scene at a time")
     ap.add_argument("--seq-scenes", type=int, default=512, help="scenes in the one-at-a-time comparison")
