@@ -466,19 +466,30 @@ __device__ __forceinline__ void inv3(const float m[3][3], float r[3][3]) {
   r[2][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) * id;
 }
 
+// The per-body constants of the solve: world inertia (xx yy zz xy) (xz yz)
+// and the inertial target.  They do not change during the passes, so the
+// sweeps load them before the lane reduction and their round trip overlaps it.
+struct BodyConst {
+  float4 w0, w1, xin, qin;
+};
+__device__ __forceinline__ BodyConst load_body_const(const Dev& d, int i) {
+  return BodyConst{d.iw0[i], d.iw1[i], d.xin[i], d.qin[i]};
+}
+
 // Inertial terms + Schur-complement solve + pose update (kernels_6dof.py:1379-1414).
-__device__ __forceinline__ void solve_body(const Dev& d, int i, float4 xi4, float4 qi, const Acc& s, float dt) {
+__device__ __forceinline__ void solve_body(const Dev& d, int i, float4 xi4, float4 qi, const Acc& s, float dt,
+                                           const BodyConst& bc) {
   float m = xi4.w;
   float idt2 = 1.0f / (dt * dt);
   float mi = m * idt2;
-  float4 w0 = d.iw0[i], w1 = d.iw1[i];  // (xx yy zz xy) (xz yz)
+  const float4 w0 = bc.w0, w1 = bc.w1;
   float I[3][3] = {{w0.x, w0.w, w1.x}, {w0.w, w0.y, w1.y}, {w1.x, w1.y, w0.z}};
   float A[3][3] = {{s.a[0] + mi, s.a[3], s.a[4]}, {s.a[3], s.a[1] + mi, s.a[5]}, {s.a[4], s.a[5], s.a[2] + mi}};
   float D[3][3] = {{I[0][0] * idt2 + s.dd[0], I[0][1] * idt2 + s.dd[3], I[0][2] * idt2 + s.dd[4]},
                    {I[1][0] * idt2 + s.dd[3], I[1][1] * idt2 + s.dd[1], I[1][2] * idt2 + s.dd[5]},
                    {I[2][0] * idt2 + s.dd[4], I[2][1] * idt2 + s.dd[5], I[2][2] * idt2 + s.dd[2]}};
   float B[3][3] = {{s.b[0], s.b[1], s.b[2]}, {s.b[3], s.b[4], s.b[5]}, {s.b[6], s.b[7], s.b[8]}};
-  float4 xin = d.xin[i], qin = d.qin[i];
+  const float4 xin = bc.xin, qin = bc.qin;
   V3 rl = V3{(xi4.x - xin.x) * mi + s.rl[0], (xi4.y - xin.y) * mi + s.rl[1], (xi4.z - xin.z) * mi + s.rl[2]};
   V3 dth = quat_to_rotvec(qmul(qi, qconj(qin)));
   V3 th = dth * idt2;
@@ -653,6 +664,8 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
         vmax = fmaxf(vmax, accumulate_group<false>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt, 0, 0, oe));
       }
     }
+    BodyConst bc{};
+    if (solve && lane == 0) bc = load_body_const(d, i);
     if (G > 1) {
 #pragma unroll
       for (int o = G / 2; o > 0; o >>= 1) {
@@ -670,7 +683,7 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
         }
       }
     }
-    if (solve && lane == 0) solve_body(d, i, xi4, qi, s, dt);
+    if (solve && lane == 0) solve_body(d, i, xi4, qi, s, dt, bc);
     int next = 0;
     if ((threadIdx.x & 31) == 0) next = nwarps + atomicAdd(counter, 1);
     chunk = __shfl_sync(0xffffffffu, next, 0);
@@ -816,6 +829,8 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
         oe = oen;
       }
     }
+    BodyConst bc{};
+    if (solve && gl == 0) bc = load_body_const(d, i);
     if (G > 1) {
 #pragma unroll
       for (int o = G / 2; o > 0; o >>= 1) {
@@ -833,7 +848,7 @@ __device__ void flag_sweep(const Dev& d, int total, int nc, int gtid, int gsize)
         }
       }
     }
-    if (solve && gl == 0) solve_body(d, i, xi4, qi, s, dt);
+    if (solve && gl == 0) solve_body(d, i, xi4, qi, s, dt, bc);
     // publish: the warp barrier orders every lane's writes (dual updates,
     // pose, finalize) before lane 0's release store, and the release is
     // cumulative over them, so one fence per body suffices (the pattern of a
