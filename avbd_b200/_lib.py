@@ -35,7 +35,7 @@ class AvbdParams(C.Structure):
                 ("record_violation", C.c_int), ("mlp_warm_start", C.c_int), ("debug_skip_arrive", C.c_int),
                 ("blocks_per_sm", C.c_int), ("timing", C.c_int), ("log_new_contacts", C.c_int),
                 ("flag_sweep", C.c_int), ("bvh_rebuild_every", C.c_int),
-                ("adaptive_lanes", C.c_int)]
+                ("adaptive_lanes", C.c_int), ("resting_floor", C.c_int)]
 
 
 class AvbdStats(C.Structure):

@@ -44,7 +44,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(C_HIST, 4, 64 * 128) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
   X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
   X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS) X(DONE, 4, N)              \
-  X(G_KEY, 8, KEYS ? G : 0) X(NODE_REC, 64, N) X(DG_OTHER, 4, 2 * DG)
+  X(G_KEY, 8, KEYS ? G : 0) X(NODE_REC, 64, N) X(DG_OTHER, 4, 2 * DG) X(FSEP, 4, N)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,
@@ -231,6 +231,7 @@ int avbd_create(const AvbdDims* dims, void* arena, size_t arena_bytes, AvbdCtx**
   d.scene_of = dims->n_scenes > 0 ? PTR(const int*, SCENE_OF) : nullptr;
   d.scene_tab = dims->n_scenes > 0 ? PTR(const float4*, SCENE_TAB) : nullptr;
   d.done = PTR(int*, DONE);
+  d.fsep = PTR(float*, FSEP);
   d.g_key = dims->anchor_keys ? PTR(unsigned long long*, G_KEY) : nullptr;
   d.ctr = PTR(DevCounters*, COUNTERS);
 #undef PTR
@@ -303,6 +304,7 @@ static void fill_devparams(AvbdCtx* c, float dt_sub) {
   q.batched = c->dims.n_scenes > 0;
   q.flag_sweep = P.flag_sweep;
   q.adaptive_lanes = P.adaptive_lanes;
+  q.resting_floor = P.resting_floor;
   q.barrier_timeout_ns = P.debug_skip_arrive ? 200000000ull : 2000000000ull;
   q.timing = P.timing;
 }

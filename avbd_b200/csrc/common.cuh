@@ -166,7 +166,8 @@ struct DevParams {
   int batched;  // bodies belong to scenes with their own dt / iterations / substeps
   int flag_sweep;  // color passes ordered by per-body completion flags instead of grid barriers
   int adaptive_lanes;  // small colors get more lanes per body (barrier sweep)
-  int pad[3];
+  int resting_floor;   // resting floor corners evaluated from the pose alone (fsep)
+  int pad[2];
 };
 
 // Phase ids of the persistent kernel's timestamps.
@@ -229,6 +230,11 @@ struct Dev {
   const float4* scene_tab;   // per scene: (substep dt, iterations, substeps per frame, 0)
   // flag-ordered sweep: passes each body has completed in this substep
   int* done;
+  // per body, the floor height when its first eight static groups are its
+  // floor corners in the resting start state (implicit corners 0-7, all rows
+  // active, no force, minimum penalties, no alpha offset), else NaN; set by
+  // predict, cleared by the sweep once a corner's state changes
+  float* fsep;
   // anchor-keyed cache (null: keys are (a, b, ordinal))
   unsigned long long* g_key;
   // counters

@@ -289,6 +289,27 @@ __device__ __forceinline__ void learned_check(const Dev& d, int kind, bool hard,
   }
 }
 
+// A copy the compiler cannot see through: known group values enter the row
+// code as runtime values, so they take the same instructions (and the same
+// FMA contractions) as values read from memory.
+__device__ __forceinline__ float opaque(float v) {
+  float r;
+  asm("mov.b32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+__device__ __forceinline__ int opaque(int v) {
+  int r;
+  asm("mov.b32 %0, %1;" : "=r"(r) : "r"(v));
+  return r;
+}
+__device__ __forceinline__ float4 opaque4(float x, float y, float z, float w) {
+  return make_float4(opaque(x), opaque(y), opaque(z), opaque(w));
+}
+// g_meta of implicit floor corner c of a hard three-row floor block.
+__device__ __forceinline__ int resting_corner_meta(int c) {
+  return make_meta(KIND_FLOOR, 1, 1, 0) | META_IMPLICIT | (c << 6);
+}
+
 // Group g's contribution to body i's system, rows in row order.  When
 // `dual` is set and body i owns g (the group's dynamic body with the lower
 // color), the previous iteration's dual update of g is applied first: both
@@ -306,12 +327,34 @@ __device__ __forceinline__ void learned_check(const Dev& d, int kind, bool hard,
 // oe: for a box-box group, its incidence entry of body i (dg_other: 2 * the
 // other body + whether i is the group's second body), so the other body is
 // known without reading the group's body pair; -1 reads the pair.
+//
+// corner >= 0: g is floor corner `corner` of a body whose corners are in the
+// resting start state (fsep: floor height fy).  While the corner stays above
+// the floor its stored state is known -- rows active, multipliers 0,
+// penalties (PEN_MIN, PEN_MIN_T, PEN_MIN_T), no alpha offset -- and its dual
+// update leaves that state as it is (the normal multiplier clamps to 0 with
+// the penalty unchanged; the friction bounds are then 0, so the friction
+// multipliers clamp to 0 and their stiffness |lambda - k C| / |C| is exactly
+// k = 1), so the group is neither read nor written: the known values go
+// through the same row code as read ones.  A corner at or below the floor is
+// read as usual; if its dual update writes it, *wrote is set.  Barrier sweep
+// only: in the flag sweep a lane's floor corner is evaluated while the index
+// of its next (box-box) group is in flight, so reading the corner costs no
+// time there, and the extra live values made the flag sweep spill (measured
+// 9 % slower).
 template <bool F>
 __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3 xi, float4 qi, bool post, bool dual,
                                                   Acc& s, float& csum, int& ccnt, int it = 0, int ci = 0,
-                                                  int oe = -1) {
-  int meta = d.g_meta[g];
-  int fl = ldm<F>(d.g_flags + g);
+                                                  int oe = -1, int corner = -1, float fy = 0.0f,
+                                                  bool* wrote = nullptr) {
+  bool rest = false;
+  if (!F && corner >= 0) {
+    float4 oa = implicit_corner(d.he[i], resting_corner_meta(corner), fy);
+    V3 rs = qrot(qi, xyz(oa));
+    rest = (xi.y + rs.y) - oa.w > 0.0f;
+  }
+  int meta = rest ? resting_corner_meta(corner) : d.g_meta[g];
+  int fl = rest ? opaque(7) : ldm<F>(d.g_flags + g);
   int kind = meta_kind(meta);
   bool three = (meta & 4) != 0, hard = (meta & 8) != 0;
   int nr = three ? 3 : 1;
@@ -337,7 +380,18 @@ __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3
       fl = ldm<F>(d.g_flags + g);  // after the owner's dual update of this pass
     }
   }
-  float4 lam = ldm<F>(d.g_lam + g), pen = ldm<F>(d.g_pen + g), ac0 = d.g_ac0[g], mat = d.g_mat[g];
+  float4 lam, pen, ac0, mat;
+  if (rest) {
+    lam = opaque4(0.0f, 0.0f, 0.0f, 0.0f);
+    pen = opaque4(PEN_MIN, PEN_MIN_T, PEN_MIN_T, 0.0f);
+    ac0 = opaque4(0.0f, 0.0f, 0.0f, 0.0f);
+    mat = opaque4(0.0f, 0.0f, FINF, fy);  // friction coefficients only scale a zero bound
+  } else {
+    lam = ldm<F>(d.g_lam + g);
+    pen = ldm<F>(d.g_pen + g);
+    ac0 = d.g_ac0[g];
+    mat = d.g_mat[g];
+  }
   float lm[3] = {lam.x, lam.y, lam.z}, pn[3] = {pen.x, pen.y, pen.z}, ac[3] = {ac0.x, ac0.y, ac0.z};
   float C[3] = {0.0f, 0.0f, 0.0f};
   V3 rs, dirs[3], dd;
@@ -391,9 +445,12 @@ __device__ __forceinline__ float accumulate_group(const Dev& d, int g, int i, V3
   if (dual && own) {
     if (fl & FL_LRN) learned_check(d, kind, hard, C, ac, lm, pn, fl);
     viol = dual_rows(kind, nr, hard, mat, C, ac, d.prm->beta, lm, pn, fl);
-    d.g_lam[g] = make_float4(lm[0], lm[1], lm[2], 0.0f);
-    d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
-    d.g_flags[g] = fl;
+    if (!rest) {
+      d.g_lam[g] = make_float4(lm[0], lm[1], lm[2], 0.0f);
+      d.g_pen[g] = make_float4(pn[0], pn[1], pn[2], 0.0f);
+      d.g_flags[g] = fl;
+      if (!F && corner >= 0) *wrote = true;
+    }
     if (kind == KIND_BOX && (fl & FL_ACT0)) {
       csum = fmaxf(csum, viol);
       ++ccnt;
@@ -647,22 +704,37 @@ __device__ void primal_color(const Dev& d, int c, PassMode pm, float dt, int gti
     Acc s;
     acc_zero(s);
     float4 qi = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    bool wrote = false;
     if (act) {
       qi = d.q[i];
       V3 xi = xyz(xi4);
       int s0 = d.sg_start[i], ns = d.sg_start[i + 1] - s0;
       int e0 = d.dg_start[i], nd = d.dg_start[i + 1] - e0;
+      // floor corners in the resting start state (fsep; an earlier pass of
+      // this substep, on any SM, may have cleared it)
+      float fy = d.prm->resting_floor ? __ldcg(d.fsep + i) : 0.0f;
+      bool rest = d.prm->resting_floor && fy == fy;
       // Issue every group record this lane will read before evaluating any,
       // so the per-group dependent loads overlap instead of chaining.
       for (int k = lane; k < ns + nd; k += G) {
-        if (k < ns) prefetch_group(d, s0 + k, false);
-        else prefetch_group(d, d.dg_idx[e0 + (k - ns)], true);
+        if (k < ns) {
+          if (!(rest && k < 8)) prefetch_group(d, s0 + k, false);
+        } else {
+          prefetch_group(d, d.dg_idx[e0 + (k - ns)], true);
+        }
       }
       for (int k = lane; k < ns + nd; k += G) {
         int g = k < ns ? s0 + k : d.dg_idx[e0 + (k - ns)];
         int oe = k < ns ? -1 : d.dg_other[e0 + (k - ns)];
-        vmax = fmaxf(vmax, accumulate_group<false>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt, 0, 0, oe));
+        vmax = fmaxf(vmax, accumulate_group<false>(d, g, i, xi, qi, pm.post, pm.dual, s, csum, ccnt, 0, 0, oe,
+                                                   rest && k < 8 ? k : -1, fy, &wrote));
       }
+    }
+    {  // a resting corner whose group was written leaves the resting state
+      constexpr unsigned BODY_LANES = G == 32 ? 0xffffffffu : (1u << G) - 1u;
+      const unsigned wmask = __ballot_sync(0xffffffffu, wrote);
+      if (lane == 0 && ((wmask >> ((threadIdx.x & 31) & ~(G - 1))) & BODY_LANES) != 0u)
+        d.fsep[i] = __int_as_float(0x7fffffff);
     }
     BodyConst bc{};
     if (solve && lane == 0) bc = load_body_const(d, i);
@@ -1136,6 +1208,33 @@ __device__ void ph_predict(const Dev& d, int gtid, int gsize) {
     bool ownb = sa || (!sb && d.color[bd.y] < d.color[bd.x]);
     int fl = d.g_flags[g];
     d.g_flags[g] = ownb ? (fl | FL_OWNB) : (fl & ~FL_OWNB);
+  }
+  if (P.resting_floor && !P.flag_sweep) {
+    // fsep: eight lanes per body, lane c checks the body's static group c
+    // (after the prelude, so this is the state the passes start from).  The
+    // trip count is a multiple of 32, so every lane of a warp runs the same
+    // iterations and the eight lanes of a body are one aligned octet.
+    const long long n8 = 8LL * d.nb, lim = (n8 + 31) & ~31LL;
+    const int lane = threadIdx.x & 31;
+    for (long long t = gtid; t < lim; t += gsize) {
+      int i = (int)(t >> 3), c = (int)(t & 7);
+      bool ok = false;
+      float fyc = 0.0f;
+      if (t < n8 && d.x[i].w > 0.0f) {  // mass in .w is never changed by predict
+        int s0 = d.sg_start[i];
+        if (d.sg_start[i + 1] - s0 >= 8) {
+          int g = s0 + c;
+          float4 lam = d.g_lam[g], pen = d.g_pen[g], ac0 = d.g_ac0[g], mat = d.g_mat[g];
+          ok = d.g_meta[g] == resting_corner_meta(c) && (d.g_flags[g] & (7 | FL_WAS | FL_LRN)) == 7 &&
+               lam.x == 0.0f && lam.y == 0.0f && lam.z == 0.0f && pen.x == PEN_MIN && pen.y == PEN_MIN_T &&
+               pen.z == PEN_MIN_T && ac0.x == 0.0f && isfinite(mat.x) && isfinite(mat.y) && isfinite(mat.w);
+          fyc = mat.w;
+        }
+      }
+      float fy0 = __shfl_sync(0xffffffffu, fyc, lane & ~7);
+      unsigned m = __ballot_sync(0xffffffffu, ok && fyc == fy0);
+      if (t < n8 && c == 0) d.fsep[i] = ((m >> lane) & 0xffu) == 0xffu ? fy0 : __int_as_float(0x7fffffff);
+    }
   }
 }
 

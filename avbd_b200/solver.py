@@ -324,6 +324,10 @@ class Solver6DOF:
         # pile, so a plain Solver6DOF(...) runs it without autotune().
         self.flag_sweep = True
         self.adaptive_lanes = False  # more lanes per body for small colors (barrier sweep)
+        # barrier sweep: floor corners resting above the floor in their start
+        # state are evaluated from the body's pose alone (same poses; fewer
+        # group reads); the flag sweep always reads them
+        self.resting_floor = True
         # LBVH rebuilt every this many substeps, refit in between (same pairs)
         self.bvh_rebuild_every = 8
         # initial dynamic-row pool (None: the reference's 192 rows per body)
@@ -816,6 +820,7 @@ class Solver6DOF:
         p.log_new_contacts = int(self._log_new)
         p.flag_sweep = int(bool(self.flag_sweep))
         p.adaptive_lanes = int(bool(self.adaptive_lanes))
+        p.resting_floor = int(bool(self.resting_floor))
         p.bvh_rebuild_every = max(1, int(self.bvh_rebuild_every))
         if self._scene_tab:  # the device loops cover the largest scene settings
             p.substeps = max(sc for sc, _ in self._scene_tab)

@@ -490,6 +490,8 @@ def run_gpu(args) -> None:
     if args.sweep:
         s.flag_sweep = args.sweep == "flags"
         s.adaptive_lanes = args.sweep == "barrier-adaptive"
+    if args.no_resting_floor:
+        s.resting_floor = False
     t_build = time.perf_counter()
     scenes.pile(s, **size)  # the caller's add_box / add_floor_contact_box / add_pin_corner calls
     t_api = time.perf_counter()
@@ -779,6 +781,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="batched bench: skip the autotuner")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start evaluation")
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-scene batched comparison key")
+    ap.add_argument("--no-resting-floor", action="store_true",
+                    help="read every floor corner group (Solver6DOF.resting_floor = False)")
     ap.add_argument("--row-capacity", type=int, default=0, help="initial dynamic-row pool (0 = reference size)")
     ap.add_argument("--batched", action="store_true", help="512 batched scenes vs one scene at a time")
     ap.add_argument("--seq-scenes", type=int, default=512, help="scenes in the one-at-a-time comparison")

@@ -102,6 +102,14 @@ typedef struct AvbdParams {
                           resident warps gets twice the lanes (repeatedly,
                           up to 32); group_size is then the lane count of
                           the large colors */
+  int resting_floor;   /* barrier sweep (flag_sweep = 0): 1 = a floor corner
+                          that rests above the floor in its substep-start
+                          state (no force, multipliers 0, minimum penalties)
+                          is evaluated from the body's pose alone, without
+                          reading or writing its group: the same sums and
+                          poses as reading it (the stored tangent multipliers
+                          may differ in the sign of zero); 0 = every group is
+                          read.  The flag sweep always reads. */
 } AvbdParams;
 
 /* Iterations whose max violation a substep records (record_violation). */
