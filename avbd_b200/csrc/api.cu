@@ -44,7 +44,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(C_HIST, 4, 64 * 128) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
   X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
   X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS) X(DONE, 4, N)              \
-  X(G_KEY, 8, KEYS ? G : 0) X(NODE_REC, 64, N) X(DG_OTHER, 4, 2 * DG) X(FSEP, 4, N)
+  X(G_KEY, 8, KEYS ? G : 0) X(NODE_REC, 128, N) X(DG_OTHER, 4, 2 * DG) X(FSEP, 4, N)
 
 enum ArrayId {
 #define X(id, sz, cnt) A_##id,

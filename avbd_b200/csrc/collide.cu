@@ -379,20 +379,45 @@ __global__ void k_lbvh_refit(const __grid_constant__ Dev d) {
   }
 }
 
-// Traversal copy of the tree: internal node p's record is four float4s,
-// (left lo, left index), (left hi, right index), (right lo), (right hi), so
-// one visit reads 64 contiguous bytes and needs no dependent load for its
-// children's boxes.  Written after every refit.
+// Traversal copy of the tree, two levels per record: internal node p's
+// record lists up to four entries -- each child that is a leaf, and the two
+// children of each child that is internal -- as (lo, code) (hi, static), 32
+// bytes each, 128 per record.  code >= 0: an internal node (descend into its
+// record); code <= -2: a leaf, body -code - 2 (no lookup of the Morton order
+// during the walk), static flag in hi.w; -1: no entry.  A walk loads half the
+// records a binary walk would.  Written after every refit.
+__device__ __forceinline__ void pack_entry(const Dev& d, int n, int c, float4* e) {
+  float4 lo = d.node_lo[c], hi = d.node_hi[c];
+  int code = c;
+  float st = 0.0f;
+  if (c >= n - 1) {
+    int b = d.order[c - (n - 1)];
+    code = -2 - b;
+    st = d.x[b].w <= 0.0f ? 1.0f : 0.0f;
+  }
+  e[0] = make_float4(lo.x, lo.y, lo.z, __int_as_float(code));
+  e[1] = make_float4(hi.x, hi.y, hi.z, st);
+}
+
 __global__ void k_lbvh_pack(const __grid_constant__ Dev d) {
   int n = d.nb;
   GSTRIDE(p, n - 1) {
-    int l = d.node_left[p], r = d.node_right[p];
-    float4 a = d.node_lo[l], b = d.node_hi[l], c = d.node_lo[r], e = d.node_hi[r];
-    float4* rec = d.node_rec + 4 * (size_t)p;
-    rec[0] = make_float4(a.x, a.y, a.z, __int_as_float(l));
-    rec[1] = make_float4(b.x, b.y, b.z, __int_as_float(r));
-    rec[2] = make_float4(c.x, c.y, c.z, 0.0f);
-    rec[3] = make_float4(e.x, e.y, e.z, 0.0f);
+    float4* rec = d.node_rec + 8 * (size_t)p;
+    int k = 0;
+    int ch[2] = {d.node_left[p], d.node_right[p]};
+    for (int a = 0; a < 2; ++a) {
+      int c = ch[a];
+      if (c >= n - 1) {
+        pack_entry(d, n, c, rec + 2 * k++);
+      } else {
+        pack_entry(d, n, d.node_left[c], rec + 2 * k++);
+        pack_entry(d, n, d.node_right[c], rec + 2 * k++);
+      }
+    }
+    for (; k < 4; ++k) {
+      rec[2 * k] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+      rec[2 * k + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
   }
 }
 
@@ -408,46 +433,46 @@ __device__ __forceinline__ void bvh_query_upper(const Dev& d, int i, F fn) {
   float4 lo = d.aabb_lo[i], hi = d.aabb_hi[i];
   bool si = d.x[i].w <= 0.0f;
   int sc = d.scene_of ? d.scene_of[i] : 0;  // batched scenes never collide with each other
-  auto leaf = [&](int node) {
-    int j = d.order[node - (n - 1)];
-    if (j > i && !(si && d.x[j].w <= 0.0f) && (!d.scene_of || d.scene_of[j] == sc)) fn(j);
+  auto report = [&](int j, bool sj) {
+    if (j > i && !(si && sj) && (!d.scene_of || d.scene_of[j] == sc)) fn(j);
   };
   if (!overlap(lo, hi, d.node_lo[0], d.node_hi[0])) return;
   if (n - 1 <= 0) {  // a single body: the root is its leaf
-    leaf(0);
+    report(d.order[0], d.x[d.order[0]].w <= 0.0f);
     return;
   }
-  // Children are tested before they are pushed: overlapping leaves are
-  // reported at once, a single overlapping inner child is descended into
-  // directly, and only the second of two is pushed.
-  int stack[64];
+  // Entries are tested before they are pushed: overlapping leaves are
+  // reported at once, the first overlapping internal entry is descended
+  // into directly, and the others are pushed.
+  constexpr int STACK = 96;
+  int stack[STACK];
   int sp = 0;
   int node = 0;
   while (true) {
-    const float4* rec = d.node_rec + 4 * (size_t)node;
-    float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
-    int l = __float_as_int(r0.w), r = __float_as_int(r1.w);
-    bool ol = overlap(lo, hi, r0, r1);
-    bool orr = overlap(lo, hi, r2, r3);
-    if (ol && l >= n - 1) {
-      leaf(l);
-      ol = false;
-    }
-    if (orr && r >= n - 1) {
-      leaf(r);
-      orr = false;
-    }
-    if (ol && orr) {
-      if (sp + 1 > 64) {
-        atomicOr(&d.ctr->err, ERR_BVH);
-        return;
+    const float4* rec = d.node_rec + 8 * (size_t)node;
+    float4 r[8];  // the whole record in one round trip
+#pragma unroll
+    for (int e = 0; e < 8; ++e) r[e] = __ldg(rec + e);
+    int next = -1;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float4 elo = r[2 * e], ehi = r[2 * e + 1];
+      int code = __float_as_int(elo.w);
+      if (code == -1 || !overlap(lo, hi, elo, ehi)) continue;
+      if (code <= -2) {
+        report(-2 - code, ehi.w != 0.0f);
+      } else if (next < 0) {
+        next = code;
+      } else {
+        if (sp + 1 > STACK) {
+          atomicOr(&d.ctr->err, ERR_BVH);
+          return;
+        }
+        stack[sp++] = code;
       }
-      stack[sp++] = r;
-      node = l;
-    } else if (ol) {
-      node = l;
-    } else if (orr) {
-      node = r;
+    }
+    if (next >= 0) {
+      node = next;
     } else {
       if (sp == 0) break;
       node = stack[--sp];
@@ -1008,11 +1033,14 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
   stage_mark(st, "k_lbvh_refit");
   k_lbvh_pack<<<grid, 256, 0, st>>>(d);
   stage_mark(st, "k_lbvh_pack");
-  k_bp_count<<<grid, 128, 0, st>>>(d);
+  // One thread per body for the walks: a walk is a chain of dependent loads,
+  // so a thread that walked twice would double the launch's duration.
+  const int walk_grid = max(grid, (d.nb + 127) / 128);
+  k_bp_count<<<walk_grid, 128, 0, st>>>(d);
   stage_mark(st, "k_bp_count");
   scan_launch(d, d.up_cnt, d.pair_start, d.nb, nullptr, nullptr, st);
   stage_mark(st, "scan_pair_offsets");
-  k_bp_fill<<<grid, 128, 0, st>>>(d);
+  k_bp_fill<<<walk_grid, 128, 0, st>>>(d);
   stage_mark(st, "k_bp_fill");
   k_narrow<<<grid, 128, 0, st>>>(d);
   stage_mark(st, "k_narrow");

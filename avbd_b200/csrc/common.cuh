@@ -199,7 +199,7 @@ struct Dev {
   int *order, *order2;
   float4 *node_lo, *node_hi;
   int *node_left, *node_right, *node_parent, *node_flag;
-  float4* node_rec;  // per internal node: both children's boxes + indices (traversal copy)
+  float4* node_rec;  // per internal node: its grandchildren's (or leaf children's) boxes (traversal copy)
   float* bounds;  // 6 floats (lo xyz, hi xyz) as ordered ints
   int *nbr_cnt, *nbr_start, *nbr_idx, *nbr_pair;
   int *up_cnt, *pair_start;

@@ -72,17 +72,19 @@ def collision_stage_bytes(n: int, pairs: int, pairs_with: int, contacts: int) ->
       k_lbvh_build (N-1) x (4 codes 16 + children/parent 16)             32 (N-1)
       k_lbvh_leaves N x (box in 32 + leaf box out 32)                     64 N
       k_lbvh_refit (N-1) x (2 child boxes 64 + box out 32)               96 (N-1)
-      k_lbvh_pack  (N-1) x (2 child boxes 64 + indices 8 + record 64)   136 (N-1)
-      k_bp_count   N x (own box 32 + count 4) + packed tree 64 (N-1)
+      k_lbvh_pack  (N-1) x (children and grandchildren indices 24 + four
+                   entry boxes 128 + leaf body and mass lookups 40 + record
+                   out 128)                                            320 (N-1)
+      k_bp_count   N x (own box 32 + count 4) + packed tree 128 (N-1)
       k_bp_fill    as k_bp_count + pairs out 8 P
       k_narrow     108 P + 140 Pc (two poses and extents, SAT / manifold out)
       k_emit       K x (3 rows x 72 + cache probe 40)                    256 K
       scans        12 B per scanned element (read twice, write once)
       k_dg_fill    4 N (zero) + K x (bodies 8) + 2K x (entry 8)     4 N + 24 K
       k_dg_sort    2K x (entry 8 read + 8 write)                          32 K"""
-    tree = 64 * max(n - 1, 0)
+    tree = 128 * max(n - 1, 0)
     return {"k_aabb": 80 * n, "k_morton": 40 * n, "radix_sort": 80 * n, "k_lbvh_build": 32 * max(n - 1, 0),
-            "k_lbvh_leaves": 64 * n, "k_lbvh_refit": 96 * max(n - 1, 0), "k_lbvh_pack": 136 * max(n - 1, 0),
+            "k_lbvh_leaves": 64 * n, "k_lbvh_refit": 96 * max(n - 1, 0), "k_lbvh_pack": 320 * max(n - 1, 0),
             "k_bp_count": 36 * n + tree, "scan_pair_offsets": 12 * n, "k_bp_fill": 36 * n + tree + 8 * pairs,
             "k_narrow": 108 * pairs + 140 * pairs_with, "scan_contact_offsets": 24 * pairs, "k_emit": 256 * contacts,
             "scan_incidence_offsets": 12 * n, "k_dg_fill": 4 * n + 24 * contacts, "k_dg_sort": 32 * contacts}
