@@ -772,9 +772,12 @@ __device__ void sat_manifold(V3 cA, M3 RA, V3 eA, V3 cB, M3 RB, V3 eB, Manifold&
 }
 
 // SAT + manifold per pair; writes the per-pair group/row counts for the scans.
+// The counters every thread adds to are summed per warp first: one atomic
+// per warp instead of one per pair on a single address.
 __global__ void k_narrow(const __grid_constant__ Dev d) {
   int np = d.ctr->n_pairs;
   float self_friction = d.prm->self_friction;
+  int creq = 0;
   GSTRIDE(p, np) {
     int2 ab = d.pair_ab[p];
     float4 xa = d.x[ab.x], xb = d.x[ab.y];
@@ -794,8 +797,10 @@ __global__ void k_narrow(const __grid_constant__ Dev d) {
     int rpc = mu <= 0.0f ? 1 : 3;
     d.pair_gcnt[p] = o.count;
     d.pair_kept[p] = o.count * rpc;  // rows requested (scanned next)
-    if (o.count) atomicAdd(&d.ctr->n_contacts_req, o.count);
+    creq += o.count;
   }
+  creq = __reduce_add_sync(0xffffffffu, creq);
+  if ((threadIdx.x & 31) == 0 && creq) atomicAdd(&d.ctr->n_contacts_req, creq);
 }
 
 // Contact-cache lookup of key k written by the previous substep's refresh.
@@ -865,6 +870,7 @@ __global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_g
   int np = d.ctr->n_pairs;
   float self_friction = d.prm->self_friction, fsm = d.prm->fsm;
   unsigned tag = epoch_tag(d.ctr->epoch);
+  int n_groups = 0, n_rows = 0, n_hits = 0, n_new = 0;  // summed per warp after the loop
   GSTRIDE(p, np) {
     int info = d.pair_info[p];
     int cnt = (info >> 6) & 7;
@@ -934,16 +940,26 @@ __global__ void k_emit(const __grid_constant__ Dev d, int dyn_row_cap, int dyn_g
         ++kept;
       }
       if (kept) {
-        atomicAdd(&d.ctr->n_dyn_groups, kept);
-        atomicAdd(&d.ctr->n_dyn_rows, kept * rpc);
+        n_groups += kept;
+        n_rows += kept * rpc;
         atomicAdd(&d.dg_cnt[ab.x], kept);
         atomicAdd(&d.dg_cnt[ab.y], kept);
       }
       if (kept < cnt) atomicOr(&d.ctr->err, ERR_ROW_OVERFLOW);
-      if (hits) atomicAdd(&d.ctr->n_cache_hits, hits);
-      if (kept - hits > 0) atomicAdd(&d.ctr->n_new_contacts, kept - hits);
+      n_hits += hits;
+      n_new += max(kept - hits, 0);
     }
     d.pair_kept[p] = kept;
+  }
+  n_groups = __reduce_add_sync(0xffffffffu, n_groups);
+  n_rows = __reduce_add_sync(0xffffffffu, n_rows);
+  n_hits = __reduce_add_sync(0xffffffffu, n_hits);
+  n_new = __reduce_add_sync(0xffffffffu, n_new);
+  if ((threadIdx.x & 31) == 0) {
+    if (n_groups) atomicAdd(&d.ctr->n_dyn_groups, n_groups);
+    if (n_rows) atomicAdd(&d.ctr->n_dyn_rows, n_rows);
+    if (n_hits) atomicAdd(&d.ctr->n_cache_hits, n_hits);
+    if (n_new) atomicAdd(&d.ctr->n_new_contacts, n_new);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     int np_ = d.ctr->n_pairs;
@@ -978,6 +994,7 @@ __global__ void k_dg_zero(const __grid_constant__ Dev d) {
 }
 
 __global__ void k_dg_sort(const __grid_constant__ Dev d) {
+  int mx = 0;  // longest list, reduced per warp after the loop
   GSTRIDE(i, d.nb) {
     int s = d.dg_start[i], e = d.dg_start[i + 1];
     for (int a = s + 1; a < e; ++a) {
@@ -991,8 +1008,10 @@ __global__ void k_dg_sort(const __grid_constant__ Dev d) {
       d.dg_idx[b + 1] = v;
       d.dg_other[b + 1] = w;
     }
-    if (e - s > 0) atomicMax(&d.ctr->max_dg, e - s);
+    mx = max(mx, e - s);
   }
+  mx = __reduce_max_sync(0xffffffffu, mx);
+  if ((threadIdx.x & 31) == 0 && mx > 0) atomicMax(&d.ctr->max_dg, mx);
 }
 
 // Empties dynamic incidence lists when self collision is off (static-only scenes).
