@@ -1047,6 +1047,17 @@ template <bool B>
 __device__ void ph_prelude(const Dev& d, int gtid, int gsize) {
   int ng = n_groups_live(d);
   for (int g = gtid; g < ng; g += gsize) {
+    // the next group's fields into L1 while this one is evaluated (a warp's
+    // six records span 16 lines, so they stay resident for one iteration)
+    const int gn = g + gsize;
+    if (gn < ng) {
+      prefetch_l1(d.g_flags + gn);
+      prefetch_l1(d.g_meta + gn);
+      prefetch_l1(d.g_body + gn);
+      prefetch_l1(d.g_lam + gn);
+      prefetch_l1(d.g_pen + gn);
+      prefetch_l1(d.g_mat + gn);
+    }
     int fl = d.g_flags[g];
     if (fl & FL_NEW) continue;  // its prelude runs in ph_mlp_prelude
     if (B && !group_on(d, g)) continue;  // batched: its scene sits this substep out
@@ -1313,10 +1324,17 @@ __device__ void ph_gate(const Dev& d, int gtid, int gsize) {
   if (d.ctr->color_dirty || P.recolor_every) return;
   int np = d.ctr->n_pairs;
   int cnt = 0;
-  for (int p = gtid; p < np; p += gsize) {
-    if (d.pair_kept[p] == 0) continue;
-    int2 ab = d.pair_ab[p];
-    if (d.color[ab.x] == d.color[ab.y]) ++cnt;
+  // two pairs per iteration, every load issued before any test (a pair's
+  // bodies are valid indices whether or not it kept contacts): two dependent
+  // round trips per pair of pairs instead of three per pair
+  for (int p = gtid; p < np; p += 2 * gsize) {
+    const int p1 = p + gsize;
+    const bool h1 = p1 < np;
+    int k0 = d.pair_kept[p], k1 = h1 ? d.pair_kept[p1] : 0;
+    int2 a0 = d.pair_ab[p], a1 = h1 ? d.pair_ab[p1] : make_int2(0, 0);
+    int c00 = d.color[a0.x], c01 = d.color[a0.y], c10 = d.color[a1.x], c11 = d.color[a1.y];
+    cnt += (k0 != 0 && c00 == c01) ? 1 : 0;
+    cnt += (k1 != 0 && c10 == c11) ? 1 : 0;
   }
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if (lane_id() == 0 && cnt) atomicAdd(&d.ctr->conflicts, cnt);
