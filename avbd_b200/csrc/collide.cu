@@ -9,6 +9,8 @@
 // Reference: solver_6dof.py:1774-1916 (driver), kernels_6dof.py:1922-2130
 // (AABB, BVH query, SAT), :2208-2537 (manifold), :2695-2912 (emission),
 // :2588-2603 (cache key/hash), :2626-2692 (CSR).
+#include <cuda/atomic>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -364,9 +366,10 @@ __global__ void k_lbvh_refit(const __grid_constant__ Dev d) {
     int p = d.node_parent[node];
     int guard = 0;
     while (p >= 0 && guard < 128) {
-      __threadfence();
-      if (atomicAdd(&d.node_flag[p], 1) == 0) break;  // first child to arrive stops
-      __threadfence();
+      // acq_rel: this thread's box store above is released with the
+      // arrival, and the second child to arrive acquires its sibling's box
+      cuda::atomic_ref<int, cuda::thread_scope_device> arrivals(d.node_flag[p]);
+      if (arrivals.fetch_add(1, cuda::memory_order_acq_rel) == 0) break;  // first child to arrive stops
       int l = d.node_left[p], r = d.node_right[p];
       float4 a = __ldcg(&d.node_lo[l]), b = __ldcg(&d.node_lo[r]);
       float4 c = __ldcg(&d.node_hi[l]), e = __ldcg(&d.node_hi[r]);
