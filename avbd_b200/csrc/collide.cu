@@ -1021,8 +1021,33 @@ __global__ void k_dg_zero(const __grid_constant__ Dev d) {
 
 __global__ void k_dg_sort(const __grid_constant__ Dev d) {
   int mx = 0;  // longest list, reduced per warp after the loop
+  constexpr int CAP = 32;  // lists up to this long are sorted in a local copy
   GSTRIDE(i, d.nb) {
     int s = d.dg_start[i], e = d.dg_start[i + 1];
+    if (e - s <= CAP) {
+      // (group, entry) packed into one key, group in the high word: group
+      // indices are unique in a body's list, so this sorts by group.  One
+      // pass of independent loads in, one pass of stores out.
+      unsigned long long kv[CAP];
+      const int n = e - s;
+      for (int k = 0; k < n; ++k)
+        kv[k] = ((unsigned long long)(unsigned)d.dg_idx[s + k] << 32) | (unsigned)d.dg_other[s + k];
+      for (int a = 1; a < n; ++a) {
+        unsigned long long v = kv[a];
+        int b = a - 1;
+        while (b >= 0 && kv[b] > v) {
+          kv[b + 1] = kv[b];
+          --b;
+        }
+        kv[b + 1] = v;
+      }
+      for (int k = 0; k < n; ++k) {
+        d.dg_idx[s + k] = (int)(kv[k] >> 32);
+        d.dg_other[s + k] = (int)(kv[k] & 0xffffffffull);
+      }
+      mx = max(mx, n);
+      continue;
+    }
     for (int a = s + 1; a < e; ++a) {
       int v = d.dg_idx[a], w = d.dg_other[a];
       int b = a - 1;
