@@ -1285,7 +1285,8 @@ __device__ void ph_collect(const Dev& d, int gtid, int gsize) {
     bool done = false;
     for (int probe = 0; probe < 4096 && !done; ++probe) {
       unsigned sl = (h + probe) & mask;
-      unsigned long long v = atomicAdd(&d.h_key[sl], 0ull);
+      // a plain L2 read: the compare-and-swap below validates it
+      unsigned long long v = __ldcg(&d.h_key[sl]);
       while (true) {
         if (v == want) {
           done = true;
