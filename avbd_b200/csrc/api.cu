@@ -40,7 +40,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
   X(NODE_RIGHT, 4, N) X(NODE_PARENT, 4, 2 * N) X(NODE_FLAG, 4, N) X(BOUNDS, 4, 8) X(UP_CNT, 4, N)              \
   X(PAIR_START, 4, N + 1) X(PAIR_AB, 8, P) X(PAIR_INFO, 4, P) X(PAIR_NRM, 16, P) X(PAIR_OFF, 16, 8 * P)        \
   X(PAIR_GCNT, 4, P) X(PAIR_GSTART, 4, P + 1) X(PAIR_RSTART, 4, P + 1) X(PAIR_KEPT, 4, P + 1) X(H_KEY, 8, H)   \
-  X(H_S0, 16, H) X(H_S1, 16, H) X(SCAN_PART, 4, SP) X(SORT_HIST, 4, SH) X(C_USED, 4, N) X(C_LOST, 4, N)        \
+  X(H_S0, 16, H) X(H_S1, 16, H) X(SCAN_PART, 4, 2 * SP) X(SORT_HIST, 4, SH) X(C_USED, 4, N) X(C_LOST, 4, N)        \
   X(C_HIST, 4, 64 * 128) X(MLP_W, 4, M) X(PARAMS, 1, (long long)sizeof(DevParams))                             \
   X(COUNTERS, 1, (long long)sizeof(DevCounters)) X(BP_TMP, 4, N * BP_SLOTS) X(NEW_LIST, 4, NC)                 \
   X(MLP_FEAT, 4, NC * MLP_IN) X(SCENE_OF, 4, NS > 0 ? N : 0) X(SCENE_TAB, 16, NS) X(DONE, 4, N)              \

@@ -153,8 +153,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total) {
   return r;
 }
 
-__global__ void k_scan_reduce(const int* in, int n_host, const int* n_dev, int* part) {
-  int n = n_dev ? *n_dev : n_host;
+__device__ __forceinline__ void scan_reduce_body(const int* in, int n, int* part) {
   int base = blockIdx.x * SCAN_CHUNK;
   int s = 0;
   if (base < n) {
@@ -174,8 +173,12 @@ __global__ void k_scan_reduce(const int* in, int n_host, const int* n_dev, int* 
   }
 }
 
+__global__ void k_scan_reduce(const int* in, int n_host, const int* n_dev, int* part) {
+  scan_reduce_body(in, n_dev ? *n_dev : n_host, part);
+}
+
 // Single block: exclusive scan of part[0..np) in place; part[np] = total.
-__global__ void k_scan_parts(int* part, int np) {
+__device__ __forceinline__ void scan_parts_body(int* part, int np) {
   __shared__ int carry;
   __shared__ int tot;
   if (threadIdx.x == 0) carry = 0;
@@ -192,9 +195,10 @@ __global__ void k_scan_parts(int* part, int np) {
   if (threadIdx.x == 0) part[np] = carry;
 }
 
-__global__ void k_scan_down(const int* in, int* out, int n_host, const int* n_dev, const int* part, int np,
-                            int* total_out) {
-  int n = n_dev ? *n_dev : n_host;
+__global__ void k_scan_parts(int* part, int np) { scan_parts_body(part, np); }
+
+__device__ __forceinline__ void scan_down_body(const int* in, int* out, int n, const int* part, int np,
+                                               int* total_out) {
   int base = blockIdx.x * SCAN_CHUNK;
   if (base > n) return;
   int i0 = base + threadIdx.x * SCAN_V;
@@ -216,6 +220,38 @@ __global__ void k_scan_down(const int* in, int* out, int n_host, const int* n_de
     out[n] = part[np];
     if (total_out) *total_out = part[np];
   }
+}
+
+__global__ void k_scan_down(const int* in, int* out, int n_host, const int* n_dev, const int* part, int np,
+                            int* total_out) {
+  scan_down_body(in, out, n_dev ? *n_dev : n_host, part, np, total_out);
+}
+
+// Two scans of the same length in one set of three launches: blockIdx.y
+// picks the array (its partials follow the first array's np + 1).
+struct Scan2 {
+  const int* in[2];
+  int* out[2];
+};
+__global__ void k_scan2_reduce(Scan2 s, int n_host, const int* n_dev, int* part, int np) {
+  const int y = blockIdx.y;
+  scan_reduce_body(s.in[y], n_dev ? *n_dev : n_host, part + y * (np + 1));
+}
+__global__ void k_scan2_parts(int* part, int np) { scan_parts_body(part + blockIdx.y * (np + 1), np); }
+__global__ void k_scan2_down(Scan2 s, int n_host, const int* n_dev, const int* part, int np) {
+  const int y = blockIdx.y;
+  scan_down_body(s.in[y], s.out[y], n_dev ? *n_dev : n_host, part + y * (np + 1), np, nullptr);
+}
+
+void scan2_launch(const Dev& d, const int* in0, int* out0, const int* in1, int* out1, int n_cap, const int* n_dev,
+                  cudaStream_t st) {
+  int np = (n_cap + SCAN_CHUNK) / SCAN_CHUNK;
+  if (np < 1) np = 1;
+  Scan2 s{{in0, in1}, {out0, out1}};
+  k_scan2_reduce<<<dim3(np, 2), SCAN_T, 0, st>>>(s, n_cap, n_dev, d.scan_part, np);
+  k_scan2_parts<<<dim3(1, 2), SCAN_T, 0, st>>>(d.scan_part, np);
+  k_scan2_down<<<dim3(np, 2), SCAN_T, 0, st>>>(s, n_cap, n_dev, d.scan_part, np);
+  g_kernel_launches += 3;
 }
 
 void scan_launch(const Dev& d, const int* in, int* out, int n_cap, const int* n_dev, int* total_out,
@@ -1115,8 +1151,7 @@ void launch_collision(Dev& d, const AvbdParams& P, const AvbdDims& dims, int gri
   k_narrow<<<grid, NARROW_BLOCK, 0, st>>>(d);
   stage_mark(st, "k_narrow");
   const int* npairs = &d.ctr->n_pairs;
-  scan_launch(d, d.pair_gcnt, d.pair_gstart, d.pair_cap, npairs, nullptr, st);
-  scan_launch(d, d.pair_kept, d.pair_rstart, d.pair_cap, npairs, nullptr, st);
+  scan2_launch(d, d.pair_gcnt, d.pair_gstart, d.pair_kept, d.pair_rstart, d.pair_cap, npairs, st);
   stage_mark(st, "scan_contact_offsets");
   k_emit<<<2 * grid, 128, 0, st>>>(d, dims.dyn_row_cap, dims.dyn_group_cap);  // 8 blocks per SM
   stage_mark(st, "k_emit");
